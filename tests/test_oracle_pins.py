@@ -1,0 +1,262 @@
+"""Pins the CPU oracle to the reference's own known-answer tests.
+
+The reference ships no golden vectors; its inline ``#[cfg(test)]`` modules and
+``tests/training_reduces_loss.rs`` are the only known answers. Each test below
+restates one of them (same inputs, same tolerance) against the oracle, so the
+oracle that later judges the CUDA path is itself held to the reference's bar.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle as O
+from tests import refcases as R
+
+
+# ---- src/math/mod.rs:215-231 ------------------------------------------------
+def test_sigmoid_logit_roundtrip():
+    for v in [-3.0, -1.0, 0.0, 1.0, 3.0]:
+        p = O.sigmoid(v)
+        assert abs(O.logit(p) - v) <= 1e-5
+
+
+def test_covariance_psd():
+    g = R.gaussian_new([0.0, 0.0, 0.0])
+    cov = O.build_cov3d(np.exp(g[R.SCL].astype(np.float64)).astype(np.float32), g[R.ROT])
+    sym = (cov + cov.T) * 0.5
+    assert np.trace(sym) > 0.0
+
+
+# ---- src/math/quaternion.rs:77-106 --------------------------------------------
+def test_identity_is_identity():
+    r = O.to_rotation_matrix([1.0, 0.0, 0.0, 0.0])
+    assert np.allclose(r, np.eye(3), atol=1e-6)
+
+
+def test_rotation_is_orthonormal():
+    r = O.to_rotation_matrix([0.5, 0.5, 0.5, 0.5])
+    assert np.allclose(r @ r.T, np.eye(3), atol=1e-5)
+
+
+def test_jacobian_matches_finite_difference():
+    q = O.quat_normalize([0.3, 0.7, -0.2, 0.5])
+    analytic = O.rotation_jacobian(q)
+    eps = np.float32(1e-4)
+    for k in range(4):
+        qp, qm = q.copy(), q.copy()
+        qp[k] += eps
+        qm[k] -= eps
+        num = (O.mat_from_quat_components(qp) - O.mat_from_quat_components(qm)) / (2 * eps)
+        diff = np.linalg.norm(analytic[k] - num)
+        assert diff < 1e-2, f"q component {k}: jacobian diff {diff}"
+
+
+# ---- src/math/covariance.rs:91-121 --------------------------------------------
+def test_cov_is_symmetric_psd():
+    cov = O.build_cov3d([0.3, 0.2, 0.5], [0.5, 0.5, 0.5, 0.5])
+    assert np.allclose(cov, cov.T, atol=1e-6)
+    assert np.linalg.det(cov.astype(np.float64)) > 0.0
+
+
+def test_scale_gradient_matches_finite_difference():
+    w = np.array([[0.7, 0.1, -0.2], [0.1, 0.4, 0.3], [-0.2, 0.3, 0.9]], np.float32)
+    log_scale = np.array([-1.0, -0.5, 0.2], np.float32)
+    rot = O.quat_normalize([0.4, 0.2, -0.7, 0.5])
+    scale = np.array([O.expf(v) for v in log_scale], np.float32)
+    d_log_scale, _ = O.backprop_cov3d(scale, rot, w)
+    eps = np.float32(1e-3)
+
+    def loss(s):
+        return float(np.sum(w * O.build_cov3d(s, rot), dtype=np.float32))
+
+    for k in range(3):
+        lp, lm = log_scale.copy(), log_scale.copy()
+        lp[k] += eps
+        lm[k] -= eps
+        sp = np.array([O.expf(v) for v in lp], np.float32)
+        sm = np.array([O.expf(v) for v in lm], np.float32)
+        num = (loss(sp) - loss(sm)) / (2 * float(eps))
+        assert abs(d_log_scale[k] - num) <= 1e-2
+
+
+# ---- src/math/sh.rs:145-156 ---------------------------------------------------
+def test_sh_dc_only():
+    c = np.zeros(48, np.float32)
+    c[0] = np.float32(1.0) / np.float32(0.28209479177387814)
+    out = O.eval_sh_deg3(c, [0.0, 0.0, 1.0])
+    assert abs(out[0] - 1.0) < 1e-5
+    assert abs(out[1] - 0.5) < 1e-5
+    assert abs(out[2] - 0.5) < 1e-5
+
+
+def test_sh_basis_grad_matches_finite_difference():
+    """Not a reference test: sh_basis_grad (sh.rs:68-89) is the derivative of sh_basis."""
+    d = np.array([0.3, -0.5, 0.81], np.float64)
+    d /= np.linalg.norm(d)
+    g = O.sh_basis_grad(d.astype(np.float32))
+    eps = 1e-3
+    for i in range(3):
+        dp, dm = d.copy(), d.copy()
+        dp[i] += eps
+        dm[i] -= eps
+        num = (O.sh_basis(dp.astype(np.float32)).astype(np.float64) - O.sh_basis(dm.astype(np.float32))) / (2 * eps)
+        assert np.allclose(g[:, i], num, atol=2e-3)
+
+
+# ---- src/cpu/backward.rs:849-856 ---------------------------------------------
+def test_ssim_of_identical_images_is_one():
+    w = h = 16
+    img = np.array([(i % 7) / 7.0 for i in range(w * h)], np.float32)
+    s, _ = O.ssim_channel(img, img, w, h)
+    assert abs(s / (w * h) - 1.0) < 1e-4
+
+
+# ---- src/cpu/backward.rs:858-892 ---------------------------------------------
+def test_image_loss_gradient_matches_finite_difference():
+    w, h = 12, 12
+    rendered, target = R.loss_grad_images(w, h)
+    lam = 0.2
+    _, grad = O.photometric_loss_grad(rendered, target, w, h, lam)
+    eps = np.float32(1e-3)
+    for (p, ch) in [(0, 0), (40, 1), (77, 2), (143, 0)]:
+        idx = p * 3 + ch
+        rp, rm = rendered.copy(), rendered.copy()
+        rp[idx] += eps
+        rm[idx] -= eps
+        lp = O.photometric_loss_grad(rp, target, w, h, lam)[0]
+        lm = O.photometric_loss_grad(rm, target, w, h, lam)[0]
+        num = np.float32(np.float32(lp) - np.float32(lm)) / (2 * eps)
+        assert abs(grad[idx] - num) < 2e-3, f"({p},{ch}): analytic {grad[idx]} vs numeric {num}"
+
+
+# ---- src/cpu/backward.rs:894-904 ---------------------------------------------
+def test_render_produces_nonblack_for_visible_gaussian():
+    cam = O.identity_camera(32, 32)
+    g = R.gaussian_new([0.0, 0.0, 2.0])
+    g[R.OPA] = R.logit(0.9)
+    g[R.SCL] = [-1.5, -1.5, -1.5]
+    g[11] = 2.0
+    img, _, _ = O.render_color(g[None], cam)
+    assert img[16, 16, 0] > 0.01
+
+
+# ---- src/cpu/backward.rs:906-982 ---------------------------------------------
+def _param_fd_check(double):
+    cam = O.identity_camera(24, 24)
+    target = R.solid_target(24, 24, [0.0, 0.0, 0.0])
+    gauss = R.fd_scene()
+    dt = np.float64 if double else np.float32
+    g0 = gauss.astype(dt)
+    out = O.render_and_backward(g0, cam, target, lambda_dssim=0.0, double=double)
+    grad = out.grads[0]
+    eps = 1e-4 if double else 1e-3
+
+    def loss_at(g):
+        return O.render_and_backward(g, cam, target, lambda_dssim=0.0, double=double).loss
+
+    def numeric(idx):
+        gp, gm = g0.copy(), g0.copy()
+        gp[0, idx] += dt(eps)
+        gm[0, idx] -= dt(eps)
+        return (loss_at(gp) - loss_at(gm)) / (2 * eps)
+
+    def check(a, n, name):
+        denom = max(abs(a), abs(n), 1e-4)
+        rel = abs(a - n) / denom
+        assert rel < 0.05 or abs(a - n) < 3e-4, f"{name}: analytic {a} vs numeric {n} (rel {rel})"
+
+    for k in range(3):
+        check(grad[R.G_POS][k], numeric(k), "d_position")
+    check(grad[R.G_OPA], numeric(3), "d_opacity")
+    for k in range(3):
+        check(grad[R.G_SCL][k], numeric(8 + k), "d_log_scale")
+    for k in [0, 1, 16, 33]:
+        check(grad[R.G_SH][k], numeric(11 + k), "d_sh")
+    q = g0[0, R.ROT].astype(np.float64)
+    num_rot = np.array([numeric(4 + k) for k in range(4)])
+
+    def proj(v):
+        v = np.asarray(v, np.float64)
+        return v - np.dot(v, q) * q
+
+    a = proj(grad[R.G_ROT])
+    nn = proj(num_rot)
+    diff = np.linalg.norm(a - nn)
+    mag = max(np.linalg.norm(nn), 1e-3)
+    assert diff / mag < 0.1, f"rotation tangential grad: analytic {a} vs numeric {nn}"
+
+
+def test_parameter_gradients_match_finite_difference():
+    _param_fd_check(double=False)
+
+
+def test_parameter_gradients_match_finite_difference_fp64():
+    _param_fd_check(double=True)
+
+
+# ---- tests/training_reduces_loss.rs:38-84 -------------------------------------
+def test_training_reduces_photometric_loss():
+    w = h = 32
+    cam = O.identity_camera(w, h)
+    target = R.solid_target(w, h, [0.2, 0.55, 0.5])
+    gs = R.training_scene()
+    cfg = O.TrainConfig()
+    adam = O.AdamState(gs.shape[0])
+    initial = O.render_and_backward(gs, cam, target, lambda_dssim=0.2).loss
+    last = initial
+    for _ in range(200):
+        out = O.render_and_backward(gs, cam, target, lambda_dssim=0.2)
+        O.adam_step(gs, out.grads, adam, cfg)
+        last = out.loss
+    assert last < initial * 0.5, f"initial {initial} -> final {last}"
+    img, _, _ = O.render_color(gs, cam)
+    for ch in range(3):
+        assert abs(img[h // 2, w // 2, ch] - target[0, 0, ch]) < 0.15
+
+
+# ---- oracle-only: exp/log routines shared with the kernels -----------------
+def _ulp_err(y, ref):
+    cr = ref.astype(np.float32)
+    lo = np.minimum(np.abs(cr), np.abs(np.nextafter(cr, np.float32(0))))
+    ulp = np.spacing(np.maximum(lo, np.float32(1e-38))).astype(np.float64)
+    return np.abs(y.astype(np.float64) - ref) / ulp
+
+
+def test_exp_cr_is_correctly_rounded():
+    rng = np.random.default_rng(0)
+    x = np.concatenate([rng.uniform(-20, 5, 300000), rng.uniform(-103, 88.7, 100000), np.linspace(-6, 0, 100001)]).astype(np.float32)
+    y = O.expf_array(x)
+    cr = np.exp(x.astype(np.float64)).astype(np.float32)
+    assert np.mean(y != cr) < 1e-5
+
+
+def test_log_cr_is_correctly_rounded():
+    rng = np.random.default_rng(1)
+    x = np.concatenate([rng.uniform(1e-6, 1.0, 200000), rng.uniform(0.5, 2.0, 200000), 10.0 ** rng.uniform(-40, 38, 100000)]).astype(np.float32)
+    y = O.logf_array(x)
+    cr = np.log(x.astype(np.float64)).astype(np.float32)
+    assert np.mean(y != cr) < 1e-5
+
+
+def test_expf_fast_accuracy():
+    rng = np.random.default_rng(2)
+    x = np.concatenate([rng.uniform(-20, 5, 300000), np.linspace(-6, 0, 200001)]).astype(np.float32)
+    y = O.expf_fast_array(x)
+    ref = np.exp(x.astype(np.float64))
+    err = _ulp_err(y, ref)
+    assert err.max() <= 0.75, f"max ulp error {err.max()}"
+    assert np.mean(y != ref.astype(np.float32)) < 0.03
+
+
+def test_exp_edge_cases():
+    assert O.expf(0.0) == 1.0
+    assert O.expf(-200.0) == 0.0
+    assert math.isinf(O.expf(100.0))
+    assert math.isnan(O.expf(float("nan")))
+    assert O.logf(1.0) == 0.0
+    assert O.logf(0.0) == -math.inf
+    assert math.isnan(O.logf(-1.0))
+    for x in (-103.0, -90.0, -87.5, 88.7, -1e-30, 1e-30):
+        xf = float(np.float32(x))
+        assert O.expf(xf) == np.float32(math.exp(xf))
