@@ -1,0 +1,213 @@
+/*
+ * rgsplat.h -- C ABI of librgsplat_b200, the B200 (sm_100a) implementation of
+ * rgsplat's differentiable 3D-Gaussian-splatting training step.
+ *
+ * Every entry point is plain C: pointers, sizes and status codes, no CUDA or
+ * torch types. Host arrays use the reference crate's own records so a Rust
+ * `extern "C"` block can pass its slices straight through:
+ *   Gaussian3D   59 x f32 (src/math/mod.rs:27-46): position[3], opacity_logit,
+ *                rotation[4] (w, x, y, z), log_scale[3], sh_coeffs[48]
+ *                (channel-major: 16 R, 16 G, 16 B).
+ *   GaussianGrad 60 x f32 (src/cpu/backward.rs:33-41): d_position[3],
+ *                d_rotation[4], d_log_scale[3], d_opacity_logit, d_sh[48],
+ *                screen_grad_norm.
+ *   Images       rendered RGB interleaved w*h*3 f32 (backward.rs:124);
+ *                targets RGBA interleaved w*h*4 f32 (TargetImage, src/io/images.rs:17-22).
+ *   AdamState    m1, m2 as [N][59] f32 in flatten_grad order
+ *                (src/pipeline/optimizer.rs:74-84, 165-173).
+ *
+ * Status: every function returns RGS_OK (0) or a negative RGS_ERR_* code; the
+ * message of the last failure on a context is rgs_last_error(ctx). Where the
+ * reference panics (NaN depth, backward.rs:191; singular c2w,
+ * src/math/mod.rs:158-159) this library returns RGS_ERR_NONFINITE /
+ * RGS_ERR_SINGULAR_CAMERA instead.
+ *
+ * Threading: a context owns one CUDA stream and its device buffers; use one
+ * context per host thread. The caller owns every host buffer.
+ */
+#ifndef RGSPLAT_H
+#define RGSPLAT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RGS_OK 0
+#define RGS_ERR_INVALID_ARG (-1)
+#define RGS_ERR_OOM (-2)
+#define RGS_ERR_CUDA (-3)
+#define RGS_ERR_NONFINITE (-4)
+#define RGS_ERR_SINGULAR_CAMERA (-5)
+#define RGS_ERR_CAPACITY (-6)
+#define RGS_ERR_NO_DEVICE (-7)
+
+#define RGS_GAUSSIAN_FLOATS 59
+#define RGS_GRAD_FLOATS 60
+
+typedef struct rgs_ctx rgs_ctx;
+
+/* Camera (src/math/mod.rs:131-145); c2w row-major, OpenCV axes (+z forward). */
+typedef struct rgs_camera {
+    uint32_t width, height;
+    float fx, fy, cx, cy;
+    float c2w[16];
+    float distortion[3]; /* carried, unused (as in the reference) */
+} rgs_camera;
+
+/* LossConfig (src/cpu/backward.rs:57-67). */
+typedef struct rgs_loss_config {
+    float lambda_dssim;
+} rgs_loss_config;
+
+/* TrainConfig (src/pipeline/optimizer.rs:22-40). */
+typedef struct rgs_train_config {
+    uint64_t num_iterations;
+    float lr_position, lr_rotation, lr_scale, lr_opacity, lr_sh_dc, lr_sh_rest;
+    float beta1, beta2, eps;
+    uint64_t densify_from_iter, densify_until_iter;
+    float densify_grad_threshold;
+    uint64_t opacity_reset_iter;
+    float prune_opacity_thresh;
+    uint64_t max_gaussians;
+} rgs_train_config;
+
+/* SplatInfo2D (src/gpu/compute.rs:64-78), 40 bytes. */
+typedef struct rgs_splat_info_2d {
+    float sx, sy, conic_a, conic_b, conic_c, color_r, color_g, color_b, alpha, depth;
+} rgs_splat_info_2d;
+
+/* AdamState (src/pipeline/optimizer.rs:74-106) as caller-owned host arrays.
+ * `len` is the number of Gaussians the arrays hold (>= n; the reference's
+ * AdamState only grows). */
+typedef struct rgs_adam_state {
+    float* m1;            /* len * 59 */
+    float* m2;            /* len * 59 */
+    float* grad_accum;    /* len */
+    uint32_t* grad_denom; /* len */
+    size_t len;
+    uint64_t t;
+} rgs_adam_state;
+
+typedef struct rgs_options {
+    int device;           /* CUDA device ordinal (default 0) */
+    int tile_w, tile_h;   /* CTA tile: 16x16 (default), 8x32 or 32x8 */
+    int batch;            /* splats staged per shared-memory round: 128, 256 (default), 512 */
+    int reference_compat; /* 1 (default): keep the reference's Adam quirks (moments are not
+                             compacted on prune, optimizer.rs:97-105; "SH DC" lr applies to
+                             flat indices 11..13, optimizer.rs:181). 0: moments follow their
+                             Gaussians and lr_sh_dc applies to sh[0], sh[16], sh[32]. */
+} rgs_options;
+
+/* Step modes of rgs_trainer_step. */
+#define RGS_STEP_PLAIN 0   /* per-view launches, host-synchronised pair counts */
+#define RGS_STEP_BATCHED 1 /* all views per stage in one launch, CUDA-graph replay */
+
+/* Projection modes of rgs_project / rgs_gpu_render. */
+#define RGS_PROJECT_WGSL 0     /* the WGSL shader's arithmetic (DC colour, its J) */
+#define RGS_PROJECT_CPU_MATH 1 /* the CPU path's projection (full SH, all culls) */
+
+/* ---- context ------------------------------------------------------------- */
+void rgs_options_default(rgs_options* opts);
+void rgs_train_config_default(rgs_train_config* cfg); /* TrainConfig::default(), optimizer.rs:42-62 */
+int rgs_create(const rgs_options* opts, rgs_ctx** out);
+void rgs_destroy(rgs_ctx* ctx);
+const char* rgs_last_error(const rgs_ctx* ctx);
+int rgs_device_count(int* count);
+int rgs_synchronize(rgs_ctx* ctx);
+
+/* ---- drop-ins for the reference's free functions (host buffers) ---------- */
+
+/* cpu::backward::render_and_backward (src/cpu/backward.rs:107-149).
+ * grads_out: n * 60 floats (may be NULL). */
+int rgs_render_and_backward(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera,
+                            const float* target_rgba, const float bg[3], const rgs_loss_config* cfg,
+                            float* loss_out, float* grads_out);
+
+/* cpu::backward::render_color (src/cpu/backward.rs:152-166): rgb_out w*h*3. */
+int rgs_render_color(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, const float bg[3],
+                     float* rgb_out);
+
+/* cpu::backward::photometric_loss_grad (src/cpu/backward.rs:646-693). */
+int rgs_photometric_loss_grad(rgs_ctx* ctx, const float* rendered_rgb, const float* target_rgba, uint32_t width,
+                              uint32_t height, float lambda, float* loss_out, float* dl_out);
+
+/* pipeline::optimizer::adam_step (src/pipeline/optimizer.rs:116-163): updates
+ * `gaussians` (n * 59) and `state` in place. grads: n * 60. */
+int rgs_adam_step(rgs_ctx* ctx, float* gaussians, size_t n, const float* grads, rgs_adam_state* state,
+                  const rgs_train_config* cfg);
+
+/* pipeline::optimizer::densify_and_prune (src/pipeline/optimizer.rs:206-272).
+ * Writes the new Gaussians to out (capacity out_cap Gaussians; 3*n always
+ * suffices) and their count to *n_out. Returns RGS_ERR_CAPACITY with *n_out
+ * set to the required count when out_cap is too small. As AdamState::resize
+ * does, the caller grows its moment arrays to *n_out if larger (never
+ * shrinking them) and zeroes grad_accum / grad_denom. */
+int rgs_densify_and_prune(rgs_ctx* ctx, const float* gaussians, size_t n, const float* grad_accum,
+                          const uint32_t* grad_denom, const rgs_train_config* cfg, float scene_extent,
+                          float* out, size_t out_cap, size_t* n_out);
+
+/* pipeline::optimizer::reset_opacities (src/pipeline/optimizer.rs:314-319). */
+int rgs_reset_opacities(rgs_ctx* ctx, float* gaussians, size_t n);
+
+/* gpu::GpuRenderer::project (src/gpu/compute.rs:140-207): one SplatInfo2D and one
+ * depth key (~bits(depth), 0xFFFFFFFF when culled) per Gaussian. */
+int rgs_project(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, int mode,
+                rgs_splat_info_2d* splats_out, uint32_t* keys_out);
+
+/* gpu::GpuRenderer::render (src/gpu/compute.rs:210-218): project, then the
+ * composite of compute.rs:243-296 (depth order, per-splat 3-sigma box from the
+ * conic, T < 1e-4 skip) on the GPU. rgb_out: w*h*3. */
+int rgs_gpu_render(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, int mode,
+                   const float bg[3], float* rgb_out);
+
+/* ---- device-resident trainer (the training loop of src/pipeline/mod.rs:203-265) */
+
+/* Upload Gaussians (n * 59); resets the Adam state (AdamState::new). */
+int rgs_trainer_set_gaussians(rgs_ctx* ctx, const float* gaussians, size_t n);
+int rgs_trainer_count(rgs_ctx* ctx, size_t* n);
+int rgs_trainer_get_gaussians(rgs_ctx* ctx, float* out, size_t cap, size_t* n_out);
+int rgs_trainer_set_cameras(rgs_ctx* ctx, const rgs_camera* cameras, size_t count);
+/* Upload camera `index`'s RGBA target (w*h*4 f32) to device memory. */
+int rgs_trainer_set_target(rgs_ctx* ctx, size_t index, const float* target_rgba);
+
+/* One training step over `nviews` camera indices: render, loss, backward,
+ * gradients summed over the views, one Adam step (denominator += nviews).
+ * losses_out: nviews floats (may be NULL). */
+int rgs_trainer_step(rgs_ctx* ctx, const uint32_t* views, size_t nviews, const float bg[3],
+                     const rgs_loss_config* loss_cfg, const rgs_train_config* train_cfg, int mode,
+                     float* losses_out);
+
+/* Render + backward only: gradients (summed over views) stay on the device
+ * for rgs_trainer_get_grads / rgs_trainer_grad_buffer / rgs_trainer_apply_adam. */
+int rgs_trainer_backward(rgs_ctx* ctx, const uint32_t* views, size_t nviews, const float bg[3],
+                         const rgs_loss_config* loss_cfg, float* losses_out);
+int rgs_trainer_get_grads(rgs_ctx* ctx, float* out /* n * 60 */);
+/* Device gradient buffer (15 float4 planes of `plane_stride` Gaussians) for a
+ * collective (e.g. an NCCL all-reduce across view-parallel ranks). */
+int rgs_trainer_grad_buffer(rgs_ctx* ctx, void** device_ptr, size_t* bytes, size_t* plane_stride);
+/* Adam over the device gradient buffer; grad_denom += denom_increment. */
+int rgs_trainer_apply_adam(rgs_ctx* ctx, const rgs_train_config* cfg, uint32_t denom_increment);
+
+int rgs_trainer_render(rgs_ctx* ctx, uint32_t view, const float bg[3], float* rgb_out);
+int rgs_trainer_densify_and_prune(rgs_ctx* ctx, const rgs_train_config* cfg, float scene_extent, size_t* n_out);
+int rgs_trainer_reset_opacities(rgs_ctx* ctx);
+int rgs_trainer_get_adam_state(rgs_ctx* ctx, rgs_adam_state* state); /* fills caller arrays (len >= count) */
+int rgs_trainer_set_adam_state(rgs_ctx* ctx, const rgs_adam_state* state);
+
+/* Statistics of the last step or render. */
+typedef struct rgs_stats {
+    uint64_t pairs;         /* (Gaussian, tile) pairs over all views */
+    uint64_t visible;       /* projected splats over all views */
+    uint64_t pair_capacity; /* pair buffer capacity (batched mode) */
+    uint32_t graph_captures;
+    uint32_t overflow_retries;
+} rgs_stats;
+int rgs_get_stats(rgs_ctx* ctx, rgs_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RGSPLAT_H */

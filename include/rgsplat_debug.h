@@ -1,0 +1,45 @@
+/*
+ * rgsplat_debug.h -- introspection entry points of librgsplat_b200.
+ *
+ * These expose the intermediate state of one view of the training step (the
+ * reference's private `project_and_bin`, `forward_pass` and `backward_pass`
+ * caches, src/cpu/backward.rs:172-512) so parity tests can compare them with a
+ * CPU restatement element by element. They are not needed to train.
+ */
+#ifndef RGSPLAT_DEBUG_H
+#define RGSPLAT_DEBUG_H
+
+#include "rgsplat.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Per-Gaussian projection (backward.rs:210-280). rec10: n * 10 floats
+ * (sx, sy, conic a, b, c, r, g, b, opacity, depth); rect4: n * 4 ints, the
+ * reference tile rectangle [tx0, ty0, tx1, ty1) (backward.rs:275-278);
+ * visible[i] = 0 when culled. */
+int rgs_debug_project(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, int32_t* visible,
+                      float* rec10, int32_t* rect4);
+
+/* Tile lists of project_and_bin (backward.rs:172-208) over the context's CTA
+ * tiles (16x16 by default), as CSR: tile t holds entries[offsets[t] ..
+ * offsets[t+1]) (Gaussian indices, front to back). offsets: tiles + 1 ints.
+ * Call with entries == NULL to get *n_pairs. */
+int rgs_debug_tile_lists(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, uint64_t* n_pairs,
+                         int32_t* offsets, int32_t* entries, size_t cap);
+
+/* forward_pass caches (backward.rs:296-385): rgb w*h*3, final T w*h, last
+ * contributor (index into the pixel's tile list, -1 if none) w*h. */
+int rgs_debug_forward(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, const float bg[3],
+                      float* rgb, float* final_t, int32_t* last);
+
+/* backward_pass output (backward.rs:391-512) merged per Gaussian: n * 9 floats
+ * (d color[3], d opacity, d conic[3], d sx, d sy), plus dL/dpixel (w*h*3). */
+int rgs_debug_backward(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, const float* target_rgba,
+                       const float bg[3], float lambda, float* acc9, float* dl_dpix);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RGSPLAT_DEBUG_H */

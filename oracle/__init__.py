@@ -211,6 +211,17 @@ def f32(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float32)
 
 
+def camera_struct(c) -> CameraStruct:
+    """CameraStruct from any object with width, height, fx, fy, cx, cy, c2w."""
+    s = CameraStruct()
+    s.width, s.height = int(c.width), int(c.height)
+    s.fx, s.fy, s.cx, s.cy = float(c.fx), float(c.fy), float(c.cx), float(c.cy)
+    flat = np.ascontiguousarray(c.c2w, dtype=np.float32).reshape(16)
+    for i in range(16):
+        s.c2w[i] = float(flat[i])
+    return s
+
+
 def set_threads(n: int) -> int:
     return lib().orc_set_threads(int(n))
 
@@ -254,7 +265,7 @@ def render_and_backward(gaussians, camera: Camera, target_rgba, bg=(0.0, 0.0, 0.
     last = np.zeros((h, w), np.int32)
     dl = np.zeros((h, w, 3), dt)
     acc = np.zeros((n, 9), dt)
-    cs = camera.struct()
+    cs = camera_struct(camera)
     if double:
         rc = lib().orc_render_and_backward_d(_d(g), n, C.byref(cs), _d(tgt), _d(bgv), float(lambda_dssim), _d(loss), _d(grads), _d(rendered), _d(final_t), _i(last), _d(dl), _d(acc))
     else:
@@ -271,7 +282,7 @@ def render_color(gaussians, camera: Camera, bg=(0.0, 0.0, 0.0)):
     ft = np.zeros((h, w), np.float32)
     lc = np.zeros((h, w), np.int32)
     bgv = f32(bg)
-    cs = camera.struct()
+    cs = camera_struct(camera)
     _check(lib().orc_render_color_f(_f(g), g.shape[0], C.byref(cs), _f(bgv), _f(rgb), _f(ft), _i(lc)), "render_color")
     return rgb, ft, lc
 
@@ -298,7 +309,7 @@ def project(gaussians, camera: Camera):
     vis = np.zeros(n, np.int32)
     rec = np.zeros((n, 16), np.float32)
     rect = np.zeros((n, 4), np.int32)
-    cs = camera.struct()
+    cs = camera_struct(camera)
     _check(lib().orc_project_f(_f(g), n, C.byref(cs), _i(vis), _f(rec), _i(rect)), "project")
     return vis, rec, rect
 
@@ -307,7 +318,7 @@ def tile_lists(gaussians, camera: Camera):
     """Tile lists of ``project_and_bin`` (backward.rs:172-208) as CSR of Gaussian indices."""
     g = f32(gaussians).reshape(-1, 59)
     n = g.shape[0]
-    cs = camera.struct()
+    cs = camera_struct(camera)
     total = C.c_int64(0)
     L = lib()
     _check(L.orc_bin_f(_f(g), n, C.byref(cs), C.byref(total), None, None, 0), "bin")
@@ -379,7 +390,7 @@ def project_wgsl(gaussians, camera: Camera):
     n = g.shape[0]
     sp = np.zeros((n, 10), np.float32)
     keys = np.zeros(n, np.uint32)
-    cs = camera.struct()
+    cs = camera_struct(camera)
     _check(lib().orc_project_wgsl_f(_f(g), n, C.byref(cs), _f(sp), _u(keys)), "project_wgsl")
     return sp, keys
 

@@ -1,0 +1,439 @@
+"""Host-side mirror of rgsplat's training-path API over the C ABI.
+
+Names, argument meanings and array layouts follow the reference crate:
+  * ``render_and_backward`` / ``render_color`` / ``photometric_loss_grad``
+    (src/cpu/backward.rs:107-166, 646-693),
+  * ``adam_step`` / ``densify_and_prune`` / ``reset_opacities`` with
+    ``AdamState`` and ``TrainConfig`` (src/pipeline/optimizer.rs),
+  * ``GpuRenderer.project`` / ``GpuRenderer.render`` (src/gpu/compute.rs:88-218),
+plus a device-resident ``Trainer`` for the training loop of
+src/pipeline/mod.rs:203-265 (plain and batched multi-view steps).
+
+Gaussians are ``(N, 59)`` float32 arrays in the ``Gaussian3D`` record order;
+gradients ``(N, 60)`` in the ``GaussianGrad`` order. Where the reference
+panics (NaN depth, singular camera) these functions raise ``RgsError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib as L
+
+GAUSSIAN_FLOATS = 59
+GRAD_FLOATS = 60
+
+
+class RgsError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{L.ERROR_NAMES.get(code, 'error')} ({code}): {message}")
+        self.code = code
+
+
+# ---------------------------------------------------------------------------
+# value types
+# ---------------------------------------------------------------------------
+@dataclass
+class Camera:
+    """``Camera`` (src/math/mod.rs:131-145): pinhole, row-major c2w, OpenCV axes."""
+
+    width: int
+    height: int
+    fx: float
+    fy: float
+    cx: float
+    cy: float
+    c2w: np.ndarray = field(default_factory=lambda: np.eye(4, dtype=np.float32))
+
+    def to_c(self) -> L.rgs_camera:
+        s = L.rgs_camera()
+        s.width, s.height = int(self.width), int(self.height)
+        s.fx, s.fy, s.cx, s.cy = float(self.fx), float(self.fy), float(self.cx), float(self.cy)
+        flat = np.ascontiguousarray(self.c2w, dtype=np.float32).reshape(16)
+        for i in range(16):
+            s.c2w[i] = float(flat[i])
+        return s
+
+    def position(self) -> np.ndarray:
+        """``Camera::position`` (mod.rs:163-165)."""
+        m = np.asarray(self.c2w, np.float32)
+        return np.array([m[0, 3], m[1, 3], m[2, 3]], np.float32)
+
+
+@dataclass
+class LossConfig:
+    """``LossConfig`` (src/cpu/backward.rs:57-67)."""
+
+    lambda_dssim: float = 0.2
+
+    def to_c(self) -> L.rgs_loss_config:
+        return L.rgs_loss_config(float(self.lambda_dssim))
+
+
+@dataclass
+class TrainConfig:
+    """``TrainConfig`` with ``Default`` (src/pipeline/optimizer.rs:22-62)."""
+
+    num_iterations: int = 30_000
+    lr_position: float = 0.00016
+    lr_rotation: float = 0.001
+    lr_scale: float = 0.005
+    lr_opacity: float = 0.05
+    lr_sh_dc: float = 0.0025
+    lr_sh_rest: float = 0.000125
+    beta1: float = 0.9
+    beta2: float = 0.999
+    eps: float = 1e-8
+    densify_from_iter: int = 500
+    densify_until_iter: int = 15_000
+    densify_grad_threshold: float = 0.0002
+    opacity_reset_iter: int = 3000
+    prune_opacity_thresh: float = 0.005
+    max_gaussians: int = 3_000_000
+
+    def to_c(self) -> L.rgs_train_config:
+        s = L.rgs_train_config()
+        for name, _ in L.rgs_train_config._fields_:
+            setattr(s, name, getattr(self, name))
+        return s
+
+
+class AdamState:
+    """``AdamState`` (src/pipeline/optimizer.rs:74-106). Arrays only ever grow."""
+
+    def __init__(self, n: int):
+        self.m1 = np.zeros(n * GAUSSIAN_FLOATS, np.float32)
+        self.m2 = np.zeros(n * GAUSSIAN_FLOATS, np.float32)
+        self.grad_accum = np.zeros(n, np.float32)
+        self.grad_denom = np.zeros(n, np.uint32)
+        self.t = 0
+
+    def __len__(self) -> int:
+        return self.grad_accum.shape[0]
+
+    def resize(self, new_n: int) -> None:
+        old = len(self)
+        if new_n > old:
+            extra = new_n - old
+            self.m1 = np.concatenate([self.m1, np.zeros(extra * GAUSSIAN_FLOATS, np.float32)])
+            self.m2 = np.concatenate([self.m2, np.zeros(extra * GAUSSIAN_FLOATS, np.float32)])
+            self.grad_accum = np.concatenate([self.grad_accum, np.zeros(extra, np.float32)])
+            self.grad_denom = np.concatenate([self.grad_denom, np.zeros(extra, np.uint32)])
+
+    def to_c(self) -> L.rgs_adam_state:
+        s = L.rgs_adam_state()
+        s.m1 = self.m1.ctypes.data_as(L.FP)
+        s.m2 = self.m2.ctypes.data_as(L.FP)
+        s.grad_accum = self.grad_accum.ctypes.data_as(L.FP)
+        s.grad_denom = self.grad_denom.ctypes.data_as(L.U32P)
+        s.len = len(self)
+        s.t = self.t
+        return s
+
+
+# ---------------------------------------------------------------------------
+# context
+# ---------------------------------------------------------------------------
+class Context:
+    """One CUDA stream plus the library's device buffers (``rgs_ctx``)."""
+
+    def __init__(self, device: int = 0, tile: tuple[int, int] = (16, 16), batch: int = 256, reference_compat: bool = True):
+        self.lib = L.load()
+        o = L.rgs_options()
+        self.lib.rgs_options_default(C.byref(o))
+        o.device = int(device)
+        o.tile_w, o.tile_h = int(tile[0]), int(tile[1])
+        o.batch = int(batch)
+        o.reference_compat = 1 if reference_compat else 0
+        h = C.c_void_p()
+        rc = self.lib.rgs_create(C.byref(o), C.byref(h))
+        if rc != L.RGS_OK:
+            raise RgsError(rc, "rgs_create failed")
+        self.handle = h
+        self.options = o
+
+    def check(self, rc: int) -> None:
+        if rc != L.RGS_OK:
+            msg = self.lib.rgs_last_error(self.handle)
+            raise RgsError(rc, msg.decode() if msg else "")
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.rgs_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def stats(self) -> dict:
+        s = L.rgs_stats()
+        self.check(self.lib.rgs_get_stats(self.handle, C.byref(s)))
+        return {name: getattr(s, name) for name, _ in L.rgs_stats._fields_}
+
+
+_tls = threading.local()
+
+
+def default_context() -> Context:
+    """The calling thread's context (the reference is called from one thread per pipeline)."""
+    ctx = getattr(_tls, "ctx", None)
+    if ctx is None:
+        ctx = Context()
+        _tls.ctx = ctx
+    return ctx
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(L.FP)
+
+
+def _gauss(g) -> np.ndarray:
+    g = _f32(g)
+    if g.size % GAUSSIAN_FLOATS:
+        raise ValueError("gaussians must be (N, 59) float32")
+    return g.reshape(-1, GAUSSIAN_FLOATS)
+
+
+def camera_c(c) -> L.rgs_camera:
+    """``rgs_camera`` from any object with width, height, fx, fy, cx, cy and a 4x4 c2w."""
+    return Camera.to_c(c)
+
+
+# ---------------------------------------------------------------------------
+# drop-ins for the reference's free functions
+# ---------------------------------------------------------------------------
+def render_and_backward(gaussians, camera: Camera, target_rgba, bg=(0.0, 0.0, 0.0), cfg: LossConfig | None = None,
+                        ctx: Context | None = None):
+    """``render_and_backward`` (src/cpu/backward.rs:107-149) -> (loss, grads (N, 60))."""
+    ctx = ctx or default_context()
+    g = _gauss(gaussians)
+    n = g.shape[0]
+    tgt = _f32(target_rgba).reshape(-1)
+    if tgt.size != camera.width * camera.height * 4:
+        raise ValueError("target must be w*h*4 RGBA floats")
+    grads = np.zeros((n, GRAD_FLOATS), np.float32)
+    loss = C.c_float(0.0)
+    bgv = _f32(bg)
+    cam = camera_c(camera)
+    lc = (cfg or LossConfig()).to_c()
+    ctx.check(ctx.lib.rgs_render_and_backward(ctx.handle, _fp(g), n, C.byref(cam), _fp(tgt), _fp(bgv), C.byref(lc), C.byref(loss), _fp(grads)))
+    return float(loss.value), grads
+
+
+def render_color(gaussians, camera: Camera, bg=(0.0, 0.0, 0.0), ctx: Context | None = None) -> np.ndarray:
+    """``render_color`` (src/cpu/backward.rs:152-166) -> interleaved RGB (H, W, 3)."""
+    ctx = ctx or default_context()
+    g = _gauss(gaussians)
+    out = np.zeros((camera.height, camera.width, 3), np.float32)
+    cam = camera_c(camera)
+    ctx.check(ctx.lib.rgs_render_color(ctx.handle, _fp(g), g.shape[0], C.byref(cam), _fp(_f32(bg)), _fp(out)))
+    return out
+
+
+def photometric_loss_grad(rendered, target_rgba, w: int, h: int, lam: float, ctx: Context | None = None):
+    """``photometric_loss_grad`` (src/cpu/backward.rs:646-693) -> (loss, dL/dpixel (w*h*3,))."""
+    ctx = ctx or default_context()
+    r = _f32(rendered).reshape(-1)
+    t = _f32(target_rgba).reshape(-1)
+    if r.size != w * h * 3 or t.size != w * h * 4:
+        raise ValueError("rendered must be w*h*3 and target w*h*4 floats")
+    dl = np.zeros(w * h * 3, np.float32)
+    loss = C.c_float(0.0)
+    ctx.check(ctx.lib.rgs_photometric_loss_grad(ctx.handle, _fp(r), _fp(t), w, h, float(lam), C.byref(loss), _fp(dl)))
+    return float(loss.value), dl
+
+
+def adam_step(gaussians: np.ndarray, grads, state: AdamState, cfg: TrainConfig, ctx: Context | None = None) -> None:
+    """``adam_step`` (src/pipeline/optimizer.rs:116-163): updates ``gaussians`` and ``state`` in place."""
+    ctx = ctx or default_context()
+    if gaussians.dtype != np.float32 or not gaussians.flags.c_contiguous:
+        raise ValueError("gaussians must be a C-contiguous float32 array (updated in place)")
+    n = gaussians.size // GAUSSIAN_FLOATS
+    gr = _f32(grads).reshape(-1, GRAD_FLOATS)
+    st = state.to_c()
+    tc = cfg.to_c()
+    ctx.check(ctx.lib.rgs_adam_step(ctx.handle, _fp(gaussians), n, _fp(gr), C.byref(st), C.byref(tc)))
+    state.t = int(st.t)
+
+
+def densify_and_prune(gaussians, state: AdamState, cfg: TrainConfig, scene_extent: float, ctx: Context | None = None) -> np.ndarray:
+    """``densify_and_prune`` (src/pipeline/optimizer.rs:206-272): returns the new Gaussians;
+    ``state`` is resized (grow only) and its densification statistics zeroed, as in the reference."""
+    ctx = ctx or default_context()
+    g = _gauss(gaussians)
+    n = g.shape[0]
+    out = np.zeros((3 * n + 1, GAUSSIAN_FLOATS), np.float32)
+    n_out = C.c_size_t(0)
+    tc = cfg.to_c()
+    ctx.check(ctx.lib.rgs_densify_and_prune(ctx.handle, _fp(g), n, _fp(state.grad_accum), state.grad_denom.ctypes.data_as(L.U32P),
+                                            C.byref(tc), float(scene_extent), _fp(out), out.shape[0], C.byref(n_out)))
+    k = int(n_out.value)
+    state.resize(k)
+    state.grad_accum[:] = 0
+    state.grad_denom[:] = 0
+    return np.ascontiguousarray(out[:k])
+
+
+def reset_opacities(gaussians: np.ndarray, ctx: Context | None = None) -> None:
+    """``reset_opacities`` (src/pipeline/optimizer.rs:314-319), in place."""
+    ctx = ctx or default_context()
+    if gaussians.dtype != np.float32 or not gaussians.flags.c_contiguous:
+        raise ValueError("gaussians must be a C-contiguous float32 array (updated in place)")
+    ctx.check(ctx.lib.rgs_reset_opacities(ctx.handle, _fp(gaussians), gaussians.size // GAUSSIAN_FLOATS))
+
+
+def estimate_scene_extent(gaussians) -> float:
+    """``estimate_scene_extent`` (src/pipeline/mod.rs:299-313): bbox diagonal."""
+    g = _gauss(gaussians)
+    if g.shape[0] == 0:
+        return 1.0
+    d = (g[:, :3].max(axis=0) - g[:, :3].min(axis=0)).astype(np.float32)
+    return float(np.float32(np.sqrt(np.float32(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]))))
+
+
+class GpuRenderer:
+    """``gpu::GpuRenderer`` (src/gpu/compute.rs:80-219) on CUDA.
+
+    ``cpu_math=False`` reproduces the shader's arithmetic (DC-only colour, its
+    column-major Jacobian); ``cpu_math=True`` returns the CPU path's splats.
+    """
+
+    def __init__(self, ctx: Context | None = None, cpu_math: bool = False):
+        self.ctx = ctx or Context()
+        self.mode = L.RGS_PROJECT_CPU_MATH if cpu_math else L.RGS_PROJECT_WGSL
+
+    def adapter_name(self) -> str:
+        return "CUDA sm_100a"
+
+    def project(self, gaussians, camera: Camera):
+        """-> (SplatInfo2D as (N, 10) float32, depth keys (N,) uint32)."""
+        g = _gauss(gaussians)
+        n = g.shape[0]
+        out = np.zeros((max(n, 1), 10), np.float32)
+        keys = np.zeros(max(n, 1), np.uint32)
+        cam = camera_c(camera)
+        self.ctx.check(self.ctx.lib.rgs_project(self.ctx.handle, _fp(g), n, C.byref(cam), self.mode,
+                                                out.ctypes.data_as(C.POINTER(L.rgs_splat_info_2d)), keys.ctypes.data_as(L.U32P)))
+        return out[:n], keys[:n]
+
+    def render(self, gaussians, camera: Camera, bg=(0.0, 0.0, 0.0)) -> np.ndarray:
+        g = _gauss(gaussians)
+        out = np.zeros((camera.height, camera.width, 3), np.float32)
+        cam = camera_c(camera)
+        self.ctx.check(self.ctx.lib.rgs_gpu_render(self.ctx.handle, _fp(g), g.shape[0], C.byref(cam), self.mode, _fp(_f32(bg)), _fp(out)))
+        return out
+
+
+# ---------------------------------------------------------------------------
+# device-resident trainer
+# ---------------------------------------------------------------------------
+class Trainer:
+    """Device-resident training state: Gaussians, Adam moments, cameras, targets."""
+
+    PLAIN = L.RGS_STEP_PLAIN
+    BATCHED = L.RGS_STEP_BATCHED
+
+    def __init__(self, gaussians, cameras: Sequence[Camera], targets=None, ctx: Context | None = None, **ctx_kwargs):
+        self.ctx = ctx or Context(**ctx_kwargs)
+        self.lib = self.ctx.lib
+        self.cameras = list(cameras)
+        self.set_gaussians(gaussians)
+        arr = (L.rgs_camera * max(len(self.cameras), 1))()
+        for i, c in enumerate(self.cameras):
+            arr[i] = camera_c(c)
+        self.ctx.check(self.lib.rgs_trainer_set_cameras(self.ctx.handle, arr, len(self.cameras)))
+        if targets is not None:
+            for i, t in enumerate(targets):
+                self.set_target(i, t)
+
+    def set_gaussians(self, gaussians) -> None:
+        g = _gauss(gaussians)
+        self.ctx.check(self.lib.rgs_trainer_set_gaussians(self.ctx.handle, _fp(g), g.shape[0]))
+
+    def set_target(self, index: int, target_rgba) -> None:
+        t = _f32(target_rgba).reshape(-1)
+        c = self.cameras[index]
+        if t.size != c.width * c.height * 4:
+            raise ValueError("target must be w*h*4 RGBA floats")
+        self.ctx.check(self.lib.rgs_trainer_set_target(self.ctx.handle, index, _fp(t)))
+
+    def __len__(self) -> int:
+        n = C.c_size_t(0)
+        self.ctx.check(self.lib.rgs_trainer_count(self.ctx.handle, C.byref(n)))
+        return int(n.value)
+
+    def gaussians(self) -> np.ndarray:
+        n = len(self)
+        out = np.zeros((max(n, 1), GAUSSIAN_FLOATS), np.float32)
+        got = C.c_size_t(0)
+        self.ctx.check(self.lib.rgs_trainer_get_gaussians(self.ctx.handle, _fp(out), out.shape[0], C.byref(got)))
+        return out[: got.value]
+
+    def step(self, views: Sequence[int], bg=(0.0, 0.0, 0.0), loss_cfg: LossConfig | None = None,
+             train_cfg: TrainConfig | None = None, mode: int = L.RGS_STEP_BATCHED) -> np.ndarray:
+        v = np.ascontiguousarray(views, dtype=np.uint32)
+        losses = np.zeros(max(v.size, 1), np.float32)
+        lc = (loss_cfg or LossConfig()).to_c()
+        tc = (train_cfg or TrainConfig()).to_c()
+        self.ctx.check(self.lib.rgs_trainer_step(self.ctx.handle, v.ctypes.data_as(L.U32P), v.size, _fp(_f32(bg)), C.byref(lc),
+                                                 C.byref(tc), int(mode), _fp(losses)))
+        return losses[: v.size]
+
+    def backward(self, views: Sequence[int], bg=(0.0, 0.0, 0.0), loss_cfg: LossConfig | None = None) -> np.ndarray:
+        v = np.ascontiguousarray(views, dtype=np.uint32)
+        losses = np.zeros(max(v.size, 1), np.float32)
+        lc = (loss_cfg or LossConfig()).to_c()
+        self.ctx.check(self.lib.rgs_trainer_backward(self.ctx.handle, v.ctypes.data_as(L.U32P), v.size, _fp(_f32(bg)), C.byref(lc), _fp(losses)))
+        return losses[: v.size]
+
+    def grads(self) -> np.ndarray:
+        out = np.zeros((max(len(self), 1), GRAD_FLOATS), np.float32)
+        self.ctx.check(self.lib.rgs_trainer_get_grads(self.ctx.handle, _fp(out)))
+        return out[: len(self)]
+
+    def grad_buffer(self):
+        """(device pointer, bytes, plane stride) of the gradient planes."""
+        p, b, s = C.c_void_p(), C.c_size_t(0), C.c_size_t(0)
+        self.ctx.check(self.lib.rgs_trainer_grad_buffer(self.ctx.handle, C.byref(p), C.byref(b), C.byref(s)))
+        return int(p.value or 0), int(b.value), int(s.value)
+
+    def apply_adam(self, train_cfg: TrainConfig | None = None, denom_increment: int = 1) -> None:
+        tc = (train_cfg or TrainConfig()).to_c()
+        self.ctx.check(self.lib.rgs_trainer_apply_adam(self.ctx.handle, C.byref(tc), int(denom_increment)))
+
+    def render(self, view: int, bg=(0.0, 0.0, 0.0)) -> np.ndarray:
+        c = self.cameras[view]
+        out = np.zeros((c.height, c.width, 3), np.float32)
+        self.ctx.check(self.lib.rgs_trainer_render(self.ctx.handle, int(view), _fp(_f32(bg)), _fp(out)))
+        return out
+
+    def densify_and_prune(self, train_cfg: TrainConfig, scene_extent: float) -> int:
+        n = C.c_size_t(0)
+        tc = train_cfg.to_c()
+        self.ctx.check(self.lib.rgs_trainer_densify_and_prune(self.ctx.handle, C.byref(tc), float(scene_extent), C.byref(n)))
+        return int(n.value)
+
+    def reset_opacities(self) -> None:
+        self.ctx.check(self.lib.rgs_trainer_reset_opacities(self.ctx.handle))
+
+    def adam_state(self) -> AdamState:
+        st = AdamState(len(self))
+        c = st.to_c()
+        self.ctx.check(self.lib.rgs_trainer_get_adam_state(self.ctx.handle, C.byref(c)))
+        st.t = int(c.t)
+        return st
+
+    def set_adam_state(self, state: AdamState) -> None:
+        c = state.to_c()
+        self.ctx.check(self.lib.rgs_trainer_set_adam_state(self.ctx.handle, C.byref(c)))

@@ -1,0 +1,187 @@
+// bin.cu -- tile binning: (CTA tile, slot) pairs in front-to-back order.
+//
+// The reference sorts visible splats by depth and then, serially, pushes each
+// splat's index into every tile its 3-sigma rectangle touches
+// (src/cpu/backward.rs:190-205). Here the depth-sorted slot order comes from
+// sort.cu; this file turns it into pairs:
+//   count scan: exclusive scan of per-slot tile counts in depth order (the
+//               total pair count stays on the device);
+//   emit:       every block expands its chunk of depth-sorted slots into
+//               (global CTA tile id, slot) pairs, load-balanced by a binary
+//               search over the sub-tile's offsets in shared memory;
+// then a stable radix sort on the tile id (sort.cu) groups the pairs by tile
+// while keeping depth order inside each tile, and `tile_ranges` records each
+// tile's [start, end).
+#include "rgs_internal.cuh"
+
+namespace rgs {
+
+constexpr int BIN_THREADS = 256;
+constexpr int BIN_SUB = 1024;  // ranks per emit sub-tile
+
+__device__ __forceinline__ void bin_chunk(uint32_t n, int G, int b, uint32_t& begin, uint32_t& end) {
+    uint32_t chunk = (uint32_t)(((uint64_t)n + G - 1) / G);
+    chunk = (chunk + 31u) & ~31u;
+    uint64_t bg = (uint64_t)chunk * b;
+    begin = (uint32_t)(bg < (uint64_t)n ? bg : (uint64_t)n);
+    end = (uint32_t)(bg + chunk < (uint64_t)n ? bg + chunk : (uint64_t)n);
+}
+
+__global__ void __launch_bounds__(BIN_THREADS) k_count_reduce(const uint32_t* __restrict__ order, const uint32_t* __restrict__ cnt,
+                                                              uint32_t S, uint32_t* __restrict__ block_sums) {
+    __shared__ uint32_t s_w[BIN_THREADS / 32];
+    uint32_t begin, end;
+    bin_chunk(S, gridDim.x, blockIdx.x, begin, end);
+    uint32_t s = 0;
+    for (uint32_t r = begin + threadIdx.x; r < end; r += BIN_THREADS) s += cnt[order[r]];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < BIN_THREADS / 32; ++w) t += s_w[w];
+        block_sums[blockIdx.x] = t;
+    }
+}
+
+// Exclusive scan of the G block sums (single block); writes the total.
+__global__ void __launch_bounds__(1024) k_scan_block_sums(uint32_t* __restrict__ block_sums, int G, uint32_t* __restrict__ total) {
+    __shared__ uint32_t s[1024];
+    __shared__ uint32_t s_carry;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    for (int base = 0; base < G; base += 1024) {
+        int i = base + threadIdx.x;
+        uint32_t v = i < G ? block_sums[i] : 0u;
+        s[threadIdx.x] = v;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {
+            uint32_t t = threadIdx.x >= o ? s[threadIdx.x - o] : 0u;
+            __syncthreads();
+            s[threadIdx.x] += t;
+            __syncthreads();
+        }
+        uint32_t incl = s[threadIdx.x];
+        if (i < G) block_sums[i] = s_carry + incl - v;
+        __syncthreads();
+        if (threadIdx.x == 1023) s_carry += incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = s_carry;
+}
+
+void launch_count_scan(const uint32_t* order, const uint32_t* cnt, uint32_t S, uint32_t* block_sums, uint32_t* total,
+                       int grid, cudaStream_t st) {
+    k_count_reduce<<<grid, BIN_THREADS, 0, st>>>(order, cnt, S, block_sums);
+    k_scan_block_sums<<<1, 1024, 0, st>>>(block_sums, grid, total);
+}
+
+__global__ void __launch_bounds__(BIN_THREADS) k_emit(const uint32_t* __restrict__ order, const uint32_t* __restrict__ cnt,
+                                                      uint32_t S, const uint32_t* __restrict__ block_sums,
+                                                      const float4* __restrict__ rec, const DevCam* __restrict__ cams,
+                                                      uint32_t n_per_view, int tile_w, int tile_h,
+                                                      uint32_t* __restrict__ pkeys, uint32_t* __restrict__ pvals,
+                                                      uint32_t cap, int* __restrict__ overflow,
+                                                      const uint32_t* __restrict__ total, uint32_t* __restrict__ eff) {
+    __shared__ uint32_t s_off[BIN_SUB + 1];
+    __shared__ uint32_t s_slot[BIN_SUB];
+    __shared__ uint32_t s_w[BIN_THREADS / 32];
+    constexpr int PER = BIN_SUB / BIN_THREADS;
+    int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    uint32_t begin, end;
+    bin_chunk(S, gridDim.x, blockIdx.x, begin, end);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *eff = min(*total, cap);
+    uint32_t base = block_sums[blockIdx.x];
+    for (uint32_t r0 = begin; r0 < end; r0 += BIN_SUB) {
+        // per-thread consecutive ranks r0 + tid*PER + k
+        uint32_t c[PER], local = 0;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            uint32_t r = r0 + (uint32_t)(tid * PER + k);
+            uint32_t slot = r < end ? order[r] : 0u;
+            c[k] = r < end ? cnt[slot] : 0u;
+            s_slot[tid * PER + k] = slot;
+            local += c[k];
+        }
+        uint32_t x = local;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) s_w[w] = x;
+        __syncthreads();
+        uint32_t wpre = 0, sub_total = 0;
+        for (int k = 0; k < BIN_THREADS / 32; ++k) {
+            uint32_t t = s_w[k];
+            if (k < w) wpre += t;
+            sub_total += t;
+        }
+        uint32_t run = wpre + x - local;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            s_off[tid * PER + k] = run;
+            run += c[k];
+        }
+        if (tid == 0) s_off[BIN_SUB] = sub_total;
+        __syncthreads();
+        for (uint32_t q = tid; q < sub_total; q += BIN_THREADS) {
+            // largest r with s_off[r] <= q (entries with zero count are skipped)
+            int lo = 0, hi = BIN_SUB - 1;
+            while (lo < hi) {
+                int mid = (lo + hi + 1) >> 1;
+                if (s_off[mid] <= q) lo = mid;
+                else hi = mid - 1;
+            }
+            uint32_t slot = s_slot[lo];
+            uint32_t j = q - s_off[lo];
+            uint32_t v = slot / n_per_view;
+            uint32_t S_ = S;
+            uint32_t rx = __float_as_uint(rec[S_ + slot].w), ry = __float_as_uint(rec[2 * (size_t)S_ + slot].w);
+            int x0 = (int)(rx & 0xffffu), x1 = (int)(rx >> 16), y0 = (int)(ry & 0xffffu);
+            int ctx0 = x0 / tile_w, ctx1 = (x1 + tile_w - 1) / tile_w, cty0 = y0 / tile_h;
+            int wt = ctx1 - ctx0;
+            int tx = ctx0 + (int)(j % (uint32_t)wt), ty = cty0 + (int)(j / (uint32_t)wt);
+            const DevCam& cm = cams[v];
+            uint32_t key = (uint32_t)(cm.tile_base + ty * cm.tiles_x + tx);
+            uint32_t out = base + q;
+            if (out < cap) {
+                pkeys[out] = key;
+                pvals[out] = slot;
+            } else {
+                *overflow = 1;
+            }
+        }
+        base += sub_total;
+        __syncthreads();
+    }
+}
+
+void launch_emit_pairs(const uint32_t* order, const uint32_t* cnt, uint32_t S, const uint32_t* block_sums, const float4* rec,
+                       const DevCam* cams, int nviews, uint32_t n_per_view, int tile_w, int tile_h, uint32_t* pair_keys,
+                       uint32_t* pair_vals, uint32_t cap, int* overflow, const uint32_t* total, uint32_t* eff, int grid,
+                       cudaStream_t st) {
+    (void)nviews;
+    k_emit<<<grid, BIN_THREADS, 0, st>>>(order, cnt, S, block_sums, rec, cams, n_per_view, tile_w, tile_h, pair_keys,
+                                         pair_vals, cap, overflow, total, eff);
+}
+
+__global__ void k_tile_ranges(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ total, uint32_t cap,
+                              uint2* __restrict__ ranges) {
+    uint32_t K = min(*total, cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < K; i += gridDim.x * blockDim.x) {
+        uint32_t t = keys[i];
+        if (i == 0 || keys[i - 1] != t) ranges[t].x = i;
+        if (i == K - 1 || keys[i + 1] != t) ranges[t].y = i + 1;
+    }
+}
+
+void launch_tile_ranges(const uint32_t* pair_keys, const uint32_t* total, uint32_t cap, uint2* ranges, cudaStream_t st) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    k_tile_ranges<<<sms * 8, 256, 0, st>>>(pair_keys, total, cap, ranges);
+}
+
+}  // namespace rgs

@@ -1,0 +1,203 @@
+// rgs_internal.cuh -- layouts and kernel launchers shared by the library's .cu files.
+//
+// HBM layout (all device-resident, SoA "planes" of float4 so every load of a
+// Gaussian's state is a coalesced 16-byte access):
+//   params  [NPL][cap] float4   plane 0: position.xyz, opacity_logit
+//                               plane 1: rotation wxyz
+//                               plane 2: log_scale.xyz, pad
+//                               planes 3..14: sh[0..47] (channel-major as in
+//                               Gaussian3D::sh_coeffs, src/math/mod.rs:45)
+//   i.e. the reference's 59-float Gaussian3D record with one pad after
+//   log_scale, transposed. Gradients and both Adam moments use the same planes;
+//   the gradient pad lane carries screen_grad_norm (backward.rs:40).
+// Per step, for V views and N Gaussians, a "slot" s = v*N + i names Gaussian i
+// as seen by view v:
+//   rec     [3][S] float4  projected splat: (sx, sy, opacity, depth),
+//                          (conic a, b, c, pixel rect x0|x1<<16),
+//                          (r, g, b, pixel rect y0|y1<<16)
+//   cnt     [S] u32        number of CTA tiles the splat touches (0 = culled)
+//   acc     [3][S] float4  blend-backward accumulators (color3, opacity,
+//                          conic3, sx, sy) of backward.rs:92-99
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+namespace rgs {
+
+constexpr int NPL = 15;        // float4 planes per Gaussian
+constexpr int NP = 59;         // trainable floats (optimizer.rs:71)
+constexpr int NG = 60;         // GaussianGrad floats (backward.rs:33-41)
+constexpr int REF_TILE = 16;   // TILE_SIZE of backward.rs:21
+
+// One view of a batch, prepared on the host.
+struct DevCam {
+    float view[12];            // rows 0..2 of inverse(c2w), row-major
+    float fx, fy, cx, cy;
+    float pos[3];              // camera centre (Camera::position, mod.rs:163-165)
+    int width, height;
+    int ref_tiles_x, ref_tiles_y;  // 16x16 reference tiles
+    int tiles_x, tiles_y;      // CTA tiles of the configured shape
+    int tile_base;             // first global CTA tile of this view
+    int pix_base;              // first pixel of this view in the batch buffers
+    int loss_base;             // first loss block of this view
+    int loss_bx;               // loss blocks per row
+    const float* target;       // RGBA float target (w*h*4), device
+};
+
+// Reference record (Gaussian3D) float index -> (plane, lane).
+__host__ __device__ inline void record_to_plane(int f, int& p, int& l) {
+    if (f < 4) { p = 0; l = f; }
+    else if (f < 8) { p = 1; l = f - 4; }
+    else if (f < 11) { p = 2; l = f - 8; }
+    else { p = 3 + (f - 11) / 4; l = (f - 11) % 4; }
+}
+
+// GaussianGrad flat index j (0..59) -> record float index (optimizer.rs:165-173,
+// 186-195); 59 (screen_grad_norm) -> the pad lane (plane 2, lane 3) = 11.
+__host__ __device__ inline int grad_to_record(int j) {
+    if (j < 3) return j;
+    if (j < 7) return 4 + (j - 3);
+    if (j < 10) return 8 + (j - 7);
+    if (j == 10) return 3;
+    if (j < 59) return j;
+    return -1;
+}
+
+enum Status {
+    RGS_OK_ = 0,
+    E_INVALID = -1,
+    E_OOM = -2,
+    E_CUDA = -3,
+    E_NONFINITE = -4,
+    E_SINGULAR = -5,
+    E_CAPACITY = -6,
+    E_NODEVICE = -7,
+};
+
+// Grow-only device allocation.
+struct DBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t need) {
+        if (need <= bytes) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        size_t want = need + need / 4 + 256;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) bytes = want;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T> T* as() const { return (T*)p; }
+};
+
+struct SortScratch {
+    DBuf hist;   // [G][R] u32
+    DBuf keys2, vals2;
+};
+
+// ---- launchers (each defined in the .cu file named in the comment) --------
+
+// layout.cu
+void launch_aos_to_planes(const float* aos, float4* planes, int n, int cap, cudaStream_t st);
+void launch_planes_to_aos(const float4* planes, float* aos, int n, int cap, cudaStream_t st);
+void launch_grads_to_aos(const float4* gplanes, float* aos, int n, int cap, int stride, cudaStream_t st);
+void launch_aos_to_grad_planes(const float* aos, float4* planes, int n, int cap, int stride, cudaStream_t st);
+void launch_check_finite(const float4* planes, int n, int cap, int* flag, cudaStream_t st);
+
+// project.cu
+void launch_project(const float4* params, int n, int cap, const DevCam* cams, int nviews,
+                    int tile_w, int tile_h, float4* rec, uint32_t* cnt, uint32_t* dkey, uint32_t* ids,
+                    cudaStream_t st);
+void launch_project_wgsl(const float4* params, int n, int cap, const DevCam* cam, int cpu_math,
+                         float* splats10, uint32_t* keys, cudaStream_t st);
+
+// sort.cu: stable LSD radix sort of (key, value) u32 pairs on bits [0, bits).
+// n_dev may be null (then n_host is used). Returns which buffer holds the
+// result: 0 = (keys, vals), 1 = (keys2, vals2) in the scratch.
+int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n_host, const uint32_t* n_dev, int bits,
+                     SortScratch& sc, int grid, cudaStream_t st, cudaError_t* err);
+int sort_grid_blocks();
+
+// bin.cu
+void launch_count_scan(const uint32_t* order, const uint32_t* cnt, uint32_t S, uint32_t* block_sums,
+                       uint32_t* total, int grid, cudaStream_t st);
+void launch_emit_pairs(const uint32_t* order, const uint32_t* cnt, uint32_t S, const uint32_t* block_sums,
+                       const float4* rec, const DevCam* cams, int nviews, uint32_t n_per_view,
+                       int tile_w, int tile_h, uint32_t* pair_keys, uint32_t* pair_vals, uint32_t cap,
+                       int* overflow, const uint32_t* total, uint32_t* eff, int grid, cudaStream_t st);
+void launch_tile_ranges(const uint32_t* pair_keys, const uint32_t* total, uint32_t cap, uint2* ranges,
+                        cudaStream_t st);
+
+// blend.cu
+struct BlendArgs {
+    const DevCam* cams;
+    int nviews;
+    const uint32_t* total_tiles;   // device scalar (or null -> total_tiles_host)
+    int total_tiles_host;
+    const uint2* ranges;
+    const uint32_t* pair_vals;
+    const float4* rec;
+    uint32_t n_per_view;
+    float bg[3];
+    float* rgb;
+    float* final_t;
+    int* last;
+    const float* dl;
+    float4* acc;
+    uint32_t* work;                // dynamic tile counter (zeroed by the launcher)
+    int rect_filter;               // per-pixel reference-tile membership test
+};
+void launch_blend_forward(const BlendArgs& a, int tile_w, int tile_h, int batch, cudaStream_t st);
+void launch_blend_backward(const BlendArgs& a, int tile_w, int tile_h, int batch, cudaStream_t st);
+
+// loss.cu
+void launch_loss(const DevCam* cams, int nviews, int total_blocks, const float* rgb, float lambda,
+                 float* dl, float* partials, float* losses, const uint32_t* total_dev,
+                 cudaStream_t st);
+
+// geom.cu
+struct AdamArgs {
+    float4* params;
+    float4* m1;
+    float4* m2;
+    float* grad_accum;
+    uint32_t* grad_denom;
+    float lr[NPL * 4];
+    float b1, b2, one_minus_b1, one_minus_b2, bc1, bc2, eps;
+    uint32_t denom_inc;
+    const int* skip_flag;   // when non-null and *skip_flag != 0 the update is skipped
+    const float* bc_dev;    // when non-null, (bc1, bc2) are read from device memory
+    int mstride;            // plane stride (Gaussians) of m1 / m2
+};
+void launch_geometry(const float4* params, int n, int cap, const DevCam* cams, int nviews,
+                     const uint32_t* cnt, const float4* acc, float4* grads, int accumulate,
+                     cudaStream_t st);
+void launch_geometry_adam(const DevCam* cams, int nviews, int n, int cap, const uint32_t* cnt,
+                          const float4* acc, const AdamArgs& a, cudaStream_t st);
+void launch_adam(int n, int cap, const float4* grads, const AdamArgs& a, cudaStream_t st);
+void launch_reset_opacities(float4* params, int n, int cap, cudaStream_t st);
+
+// densify.cu
+struct DensifyArgs {
+    const float4* params;
+    int n, cap;
+    const float* grad_accum;
+    const uint32_t* grad_denom;
+    float prune_opacity, grad_threshold, extent;
+    uint64_t max_gaussians;
+};
+// Writes the new Gaussians into `out` (grown as needed; its plane stride is
+// returned in *out_cap) and the new count in *n_out. Synchronises `st`.
+cudaError_t densify_and_prune(const DensifyArgs& a, DBuf& out, int* out_cap, DBuf& scratch,
+                              int* n_out, cudaStream_t st);
+
+}  // namespace rgs

@@ -1,0 +1,241 @@
+// rgs_math.cuh -- device math shared by every kernel of the training path.
+//
+// Every expression below that feeds an integer decision (the 3-sigma AABB
+// truncation of src/math/projection.rs:138-165, the culls of
+// src/cpu/backward.rs:220-250) or a threshold test (alpha >= 1/255, T < 1e-4,
+// backward.rs:341-355) is written as the same sequence of IEEE-754 roundings
+// the reference evaluates: the translation units are compiled with
+// --fmad=false so no a*b+c is fused, and fma is used only where written
+// explicitly. The transcendental routines are the library's own (the
+// reference calls libm):
+//   * rgs_exp_cr / rgs_log_cr: double-precision Cody-Waite reduction with
+//     fdlibm's two-part ln2, Taylor polynomial (degree 13 for exp; log through
+//     2*atanh(s) up to s^21), one rounding to float. Correctly rounded except
+//     with probability ~1e-8, so they agree with glibc's expf/logf wherever
+//     those are correctly rounded. Used once per Gaussian.
+//   * rgs_expf_fast: single-precision Cody-Waite + degree-8 Taylor with a
+//     compensated final sum (max error 0.62 ulp). Used per (pixel, splat).
+#pragma once
+#include <cstdint>
+
+#define RGS_HD __host__ __device__ __forceinline__
+
+namespace rgs {
+
+__device__ __forceinline__ double exp_core_d(double x) {
+    const double LN2_HI = 6.93147180369123816490e-01;
+    const double LN2_LO = 1.90821492927058770002e-10;
+    const double INV_LN2 = 1.44269504088896338700e+00;
+    const double SHIFT = 6755399441055744.0;
+    double j = fma(x, INV_LN2, SHIFT);
+    double k = j - SHIFT;
+    double r = fma(-k, LN2_HI, x);
+    r = fma(-k, LN2_LO, r);
+    double p = 1.0 / 6227020800.0;
+    p = fma(p, r, 1.0 / 479001600.0);
+    p = fma(p, r, 1.0 / 39916800.0);
+    p = fma(p, r, 1.0 / 3628800.0);
+    p = fma(p, r, 1.0 / 362880.0);
+    p = fma(p, r, 1.0 / 40320.0);
+    p = fma(p, r, 1.0 / 5040.0);
+    p = fma(p, r, 1.0 / 720.0);
+    p = fma(p, r, 1.0 / 120.0);
+    p = fma(p, r, 1.0 / 24.0);
+    p = fma(p, r, 1.0 / 6.0);
+    p = fma(p, r, 0.5);
+    p = fma(p, r, 1.0);
+    p = fma(p, r, 1.0);
+    int ki = (int)k;
+    return p * __longlong_as_double((long long)(ki + 1023) << 52);
+}
+
+__device__ __forceinline__ float exp_cr(float x) {
+    if (x != x) return x + x;
+    if (x > 88.7228394f) return __int_as_float(0x7f800000);
+    if (x < -103.972084f) return 0.0f;
+    return __double2float_rn(exp_core_d((double)x));
+}
+
+__device__ __forceinline__ float log_cr(float x) {
+    if (x != x) return x + x;
+    if (x < 0.0f) return __int_as_float(0x7fc00000);
+    if (x == 0.0f) return __int_as_float(0xff800000);
+    if (x == __int_as_float(0x7f800000)) return x;
+    const double LN2_HI = 6.93147180369123816490e-01;
+    const double LN2_LO = 1.90821492927058770002e-10;
+    double d = (double)x;
+    unsigned long long b = (unsigned long long)__double_as_longlong(d);
+    int e = (int)((b >> 52) & 0x7ffull) - 1023;
+    double m = __longlong_as_double((long long)((b & 0x000fffffffffffffull) | 0x3ff0000000000000ull));
+    if (m > 1.4142135623730951) { m = m * 0.5; e += 1; }
+    double f = m - 1.0;
+    double s = f / (2.0 + f);
+    double z = s * s;
+    double P = 2.0 / 21.0;
+    P = fma(P, z, 2.0 / 19.0);
+    P = fma(P, z, 2.0 / 17.0);
+    P = fma(P, z, 2.0 / 15.0);
+    P = fma(P, z, 2.0 / 13.0);
+    P = fma(P, z, 2.0 / 11.0);
+    P = fma(P, z, 2.0 / 9.0);
+    P = fma(P, z, 2.0 / 7.0);
+    P = fma(P, z, 2.0 / 5.0);
+    P = fma(P, z, 2.0 / 3.0);
+    double logm = fma(s * z, P, 2.0 * s);
+    double ef = (double)e;
+    double r = ef * LN2_HI + fma(ef, LN2_LO, logm);
+    return __double2float_rn(r);
+}
+
+__device__ __forceinline__ float expf_fast(float x) {
+    if (x != x) return x + x;
+    if (x > 88.7228394f) return __int_as_float(0x7f800000);
+    if (x < -103.972084f) return 0.0f;
+    const float L2E = 1.44269502f;
+    const float SHIFT = 12582912.0f;
+    const float LN2_HI = 0.693145751953125f;
+    const float LN2_LO = 1.42860677e-06f;
+    float j = __fmaf_rn(x, L2E, SHIFT);
+    float k = j - SHIFT;
+    float rh = __fmaf_rn(-k, LN2_HI, x);
+    float rl = -k * LN2_LO;
+    float q = 2.48015873e-05f;
+    q = __fmaf_rn(q, rh, 1.98412698e-4f);
+    q = __fmaf_rn(q, rh, 1.38888889e-3f);
+    q = __fmaf_rn(q, rh, 8.33333333e-3f);
+    q = __fmaf_rn(q, rh, 4.16666667e-2f);
+    q = __fmaf_rn(q, rh, 1.66666667e-1f);
+    q = __fmaf_rn(q, rh, 0.5f);
+    float hi = 1.0f + rh;
+    float lo = (1.0f - hi) + rh;
+    float s = rh * rh;
+    float tail = __fmaf_rn(s, q, lo);
+    float ea = hi + tail;
+    tail = __fmaf_rn(rl, ea, tail);
+    float p = hi + tail;
+    int ki = (int)k;
+    if (ki > 127) return (p * __int_as_float(254 << 23)) * __int_as_float(ki << 23);
+    if (ki < -126) return (p * __int_as_float(1 << 23)) * __int_as_float((ki + 253) << 23);
+    return p * __int_as_float((ki + 127) << 23);
+}
+
+// Rust f32::max / f32::min ignore a NaN operand (fmaxf/fminf do the same);
+// f32::clamp propagates NaN.
+__device__ __forceinline__ float rclamp(float x, float lo, float hi) {
+    if (x < lo) x = lo;
+    if (x > hi) x = hi;
+    return x;
+}
+
+// Rust `f as i32`: truncate toward zero, saturate, NaN -> 0.
+__device__ __forceinline__ int as_i32(float f) {
+    if (f != f) return 0;
+    if (f >= 2147483647.0f) return 2147483647;
+    if (f <= -2147483648.0f) return (int)0x80000000;
+    return (int)f;
+}
+
+__device__ __forceinline__ float sigmoid(float x) { return 1.0f / (1.0f + exp_cr(-x)); }
+__device__ __forceinline__ float logit(float p) { return log_cr(p / (1.0f - p)); }
+
+struct M3 {
+    float m[3][3];
+};
+
+__device__ __forceinline__ M3 mul(const M3& a, const M3& b) {
+    M3 c;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) c.m[i][j] = (a.m[i][0] * b.m[0][j] + a.m[i][1] * b.m[1][j]) + a.m[i][2] * b.m[2][j];
+    return c;
+}
+__device__ __forceinline__ M3 tr(const M3& a) {
+    M3 c;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) c.m[i][j] = a.m[j][i];
+    return c;
+}
+
+// quaternion.rs:10-17 followed by quaternion.rs:23-30.
+__device__ __forceinline__ void qnormalize(const float q[4], float o[4]) {
+    float n = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    if (n < 1e-12f) { o[0] = 1.0f; o[1] = 0.0f; o[2] = 0.0f; o[3] = 0.0f; }
+    else { o[0] = q[0] / n; o[1] = q[1] / n; o[2] = q[2] / n; o[3] = q[3] / n; }
+}
+__device__ __forceinline__ M3 mat_from_quat(const float q[4]) {
+    float w = q[0], x = q[1], y = q[2], z = q[3];
+    M3 r;
+    r.m[0][0] = 1.0f - 2.0f * (y * y + z * z); r.m[0][1] = 2.0f * (x * y - w * z); r.m[0][2] = 2.0f * (x * z + w * y);
+    r.m[1][0] = 2.0f * (x * y + w * z); r.m[1][1] = 1.0f - 2.0f * (x * x + z * z); r.m[1][2] = 2.0f * (y * z - w * x);
+    r.m[2][0] = 2.0f * (x * z - w * y); r.m[2][1] = 2.0f * (y * z + w * x); r.m[2][2] = 1.0f - 2.0f * (x * x + y * y);
+    return r;
+}
+__device__ __forceinline__ M3 to_rotation_matrix(const float q[4]) {
+    float n[4];
+    qnormalize(q, n);
+    return mat_from_quat(n);
+}
+// covariance.rs:16-31: M = R diag(s), Sigma = M M^T.
+__device__ __forceinline__ M3 rs_matrix(const float s[3], const float q[4]) {
+    M3 r = to_rotation_matrix(q), o;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) o.m[i][j] = r.m[i][j] * s[j];
+    return o;
+}
+__device__ __forceinline__ M3 build_cov3d(const float s[3], const float q[4]) {
+    M3 m = rs_matrix(s, q);
+    return mul(m, tr(m));
+}
+
+// Constants of src/math/sh.rs:9-32, parsed straight to f32 as Rust does.
+#define SH_C0 0.28209479177387814f
+#define SH_C1 0.4886025119029199f
+#define SH_C2_0 1.0925484305920792f
+#define SH_C2_1 -1.0925484305920792f
+#define SH_C2_2 0.31539156525252005f
+#define SH_C2_3 -1.0925484305920792f
+#define SH_C2_4 0.5462742152960396f
+#define SH_C3_0 -0.5900435899266435f
+#define SH_C3_1 2.890611442640554f
+#define SH_C3_2 -0.4570457994644658f
+#define SH_C3_3 0.3731763325901154f
+#define SH_C3_4 -0.4570457994644658f
+#define SH_C3_5 1.445305721320277f
+#define SH_C3_6 -0.5900435899266435f
+
+// sh.rs:39-61
+__device__ __forceinline__ void sh_basis(const float d[3], float b[16]) {
+    float x = d[0], y = d[1], z = d[2];
+    float xx = x * x, yy = y * y, zz = z * z, xy = x * y, xz = x * z, yz = y * z;
+    b[0] = SH_C0;
+    b[1] = SH_C1 * -y;
+    b[2] = SH_C1 * z;
+    b[3] = SH_C1 * -x;
+    b[4] = SH_C2_0 * xy;
+    b[5] = SH_C2_1 * yz;
+    b[6] = SH_C2_2 * (2.0f * zz - xx - yy);
+    b[7] = SH_C2_3 * xz;
+    b[8] = SH_C2_4 * (xx - yy);
+    b[9] = SH_C3_0 * y * (3.0f * xx - yy);
+    b[10] = SH_C3_1 * xy * z;
+    b[11] = SH_C3_2 * y * (4.0f * zz - xx - yy);
+    b[12] = SH_C3_3 * z * (2.0f * zz - 3.0f * xx - 3.0f * yy);
+    b[13] = SH_C3_4 * x * (4.0f * zz - xx - yy);
+    b[14] = SH_C3_5 * z * (xx - yy);
+    b[15] = SH_C3_6 * x * (xx - 3.0f * yy);
+}
+
+// sh.rs:122-139: normalize(cam - pos), [0,0,1] when shorter than 1e-8.
+__device__ __forceinline__ void view_dir(const float gp[3], const float cp[3], float d[3]) {
+    float v0 = cp[0] - gp[0], v1 = cp[1] - gp[1], v2 = cp[2] - gp[2];
+    float len = sqrtf(v0 * v0 + v1 * v1 + v2 * v2);
+    if (len < 1e-8f) { d[0] = 0.0f; d[1] = 0.0f; d[2] = 1.0f; }
+    else { d[0] = v0 / len; d[1] = v1 / len; d[2] = v2 / len; }
+}
+
+}  // namespace rgs

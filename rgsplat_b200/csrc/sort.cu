@@ -1,0 +1,243 @@
+// sort.cu -- stable LSD radix sort of (u32 key, u32 value) pairs.
+//
+// Replaces the reference's serial `sort_unstable_by` on depth plus the serial
+// per-tile push loop (src/cpu/backward.rs:190-205). Stability is what makes
+// the result deterministic: inputs arrive in slot order, so equal keys keep
+// index order, which is the (tile, depth bits, index) order the oracle uses.
+//
+// Each pass is reduce-then-scan with a fixed grid (no inter-block waiting, so
+// nothing can spin): every block owns one contiguous chunk of the input.
+//   upsweep:   per-block digit histogram of its chunk          -> hist[b][d]
+//   scan:      one block turns hist into global offsets (digit-major order)
+//   downsweep: each block walks its chunk in 2048-key sub-tiles, ranks keys
+//              stably (warp match_any + per-warp counters), reorders the
+//              sub-tile in shared memory by digit and writes it out with
+//              consecutive threads hitting consecutive addresses.
+// The element count may live in device memory (pair counts are produced on
+// the GPU), so the whole sort can be captured in a CUDA graph.
+#include "rgs_internal.cuh"
+
+namespace rgs {
+
+constexpr int SORT_THREADS = 256;
+constexpr int SORT_WARPS = SORT_THREADS / 32;
+constexpr int SORT_IPT = 8;
+constexpr int SORT_TILE = SORT_THREADS * SORT_IPT;
+
+__device__ __forceinline__ uint32_t load_n(const uint32_t* n_dev, uint32_t n_host) { return n_dev ? *n_dev : n_host; }
+
+__device__ __forceinline__ void chunk_of(uint32_t n, int G, int b, uint32_t& begin, uint32_t& end) {
+    uint32_t chunk = (uint32_t)(((uint64_t)n + G - 1) / G);
+    chunk = (chunk + 31u) & ~31u;
+    uint64_t bg = (uint64_t)chunk * b;
+    begin = (uint32_t)(bg < (uint64_t)n ? bg : (uint64_t)n);
+    end = (uint32_t)(bg + chunk < (uint64_t)n ? bg + chunk : (uint64_t)n);
+}
+
+template <int BITS>
+__global__ void __launch_bounds__(SORT_THREADS) k_upsweep(const uint32_t* __restrict__ keys, const uint32_t* n_dev,
+                                                          uint32_t n_host, int shift, uint32_t* __restrict__ hist) {
+    constexpr int R = 1 << BITS;
+    __shared__ uint32_t s_h[SORT_WARPS][R];
+    int tid = threadIdx.x, w = tid >> 5;
+    for (int i = tid; i < SORT_WARPS * R; i += SORT_THREADS) (&s_h[0][0])[i] = 0;
+    __syncthreads();
+    uint32_t n = load_n(n_dev, n_host), begin, end;
+    chunk_of(n, gridDim.x, blockIdx.x, begin, end);
+    for (uint32_t p = begin + tid; p < end; p += SORT_THREADS) {
+        uint32_t d = (keys[p] >> shift) & (R - 1);
+        atomicAdd(&s_h[w][d], 1u);
+    }
+    __syncthreads();
+    for (int d = tid; d < R; d += SORT_THREADS) {
+        uint32_t s = 0;
+#pragma unroll
+        for (int k = 0; k < SORT_WARPS; ++k) s += s_h[k][d];
+        hist[(size_t)blockIdx.x * R + d] = s;
+    }
+}
+
+// Block-wide exclusive scan of R values held D = R/256 per thread (consecutive).
+template <int D>
+__device__ __forceinline__ void block_exclusive_scan(uint32_t (&v)[D], uint32_t* s_warp, uint32_t& total) {
+    int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    uint32_t local = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) { uint32_t t = v[k]; v[k] = local; local += t; }
+    uint32_t x = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        uint32_t t = lane < SORT_WARPS ? s_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        if (lane < SORT_WARPS) s_warp[lane] = t;
+    }
+    __syncthreads();
+    uint32_t warp_prefix = w > 0 ? s_warp[w - 1] : 0;
+    total = s_warp[SORT_WARPS - 1];
+    uint32_t excl = warp_prefix + x - local;
+#pragma unroll
+    for (int k = 0; k < D; ++k) v[k] += excl;
+    __syncthreads();
+}
+
+template <int BITS>
+__global__ void __launch_bounds__(SORT_THREADS) k_scan_hist(uint32_t* __restrict__ hist, int G) {
+    constexpr int R = 1 << BITS;
+    constexpr int D = R / SORT_THREADS;
+    __shared__ uint32_t s_warp[SORT_WARPS];
+    int tid = threadIdx.x;
+    uint32_t tot[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        int d = tid * D + k;
+        uint32_t s = 0;
+        for (int b = 0; b < G; ++b) s += hist[(size_t)b * R + d];
+        tot[k] = s;
+    }
+    uint32_t total;
+    block_exclusive_scan<D>(tot, s_warp, total);
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        int d = tid * D + k;
+        uint32_t run = tot[k];
+        for (int b = 0; b < G; ++b) {
+            uint32_t c = hist[(size_t)b * R + d];
+            hist[(size_t)b * R + d] = run;
+            run += c;
+        }
+    }
+}
+
+template <int BITS>
+__global__ void __launch_bounds__(SORT_THREADS) k_downsweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+                                                            uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                            const uint32_t* n_dev, uint32_t n_host, int shift,
+                                                            const uint32_t* __restrict__ hist) {
+    constexpr int R = 1 << BITS;
+    constexpr int D = R / SORT_THREADS;
+    __shared__ uint32_t s_run[R];
+    __shared__ uint32_t s_wcnt[SORT_WARPS][R];
+    __shared__ uint32_t s_dstart[R];
+    __shared__ uint32_t s_tot[R];
+    __shared__ uint32_t s_warp[SORT_WARPS];
+    __shared__ uint32_t s_keys[SORT_TILE];
+    __shared__ uint32_t s_vals[SORT_TILE];
+    int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    uint32_t n = load_n(n_dev, n_host), begin, end;
+    chunk_of(n, gridDim.x, blockIdx.x, begin, end);
+    for (int d = tid; d < R; d += SORT_THREADS) s_run[d] = hist[(size_t)blockIdx.x * R + d];
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    for (uint32_t base = begin; base < end; base += SORT_TILE) {
+        for (int i = tid; i < SORT_WARPS * R; i += SORT_THREADS) (&s_wcnt[0][0])[i] = 0;
+        __syncthreads();
+        uint32_t k[SORT_IPT], v[SORT_IPT], rank[SORT_IPT];
+        int dig[SORT_IPT];
+#pragma unroll
+        for (int i = 0; i < SORT_IPT; ++i) {
+            uint32_t pos = base + (uint32_t)(w * 32 * SORT_IPT + i * 32 + lane);
+            bool valid = pos < end;
+            k[i] = valid ? kin[pos] : 0u;
+            v[i] = valid ? vin[pos] : 0u;
+            dig[i] = valid ? (int)((k[i] >> shift) & (R - 1)) : R;
+        }
+#pragma unroll
+        for (int i = 0; i < SORT_IPT; ++i) {
+            unsigned peers = __match_any_sync(0xffffffffu, dig[i]);
+            int leader = __ffs(peers) - 1;
+            uint32_t before = dig[i] < R ? s_wcnt[w][dig[i]] : 0u;
+            __syncwarp();
+            if (dig[i] < R && lane == leader) s_wcnt[w][dig[i]] = before + __popc(peers);
+            __syncwarp();
+            rank[i] = before + __popc(peers & lt_mask);
+        }
+        __syncthreads();
+        uint32_t tot[D];
+#pragma unroll
+        for (int q = 0; q < D; ++q) {
+            int d = tid * D + q;
+            uint32_t acc = 0;
+#pragma unroll
+            for (int ww = 0; ww < SORT_WARPS; ++ww) {
+                uint32_t c = s_wcnt[ww][d];
+                s_wcnt[ww][d] = acc;
+                acc += c;
+            }
+            tot[q] = acc;
+            s_tot[d] = acc;
+        }
+        uint32_t total;
+        block_exclusive_scan<D>(tot, s_warp, total);
+#pragma unroll
+        for (int q = 0; q < D; ++q) s_dstart[tid * D + q] = tot[q];
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < SORT_IPT; ++i) {
+            if (dig[i] < R) {
+                uint32_t lp = s_dstart[dig[i]] + s_wcnt[w][dig[i]] + rank[i];
+                s_keys[lp] = k[i];
+                s_vals[lp] = v[i];
+            }
+        }
+        __syncthreads();
+        uint32_t cnt = min((uint32_t)SORT_TILE, end - base);
+        for (uint32_t j = tid; j < cnt; j += SORT_THREADS) {
+            uint32_t key = s_keys[j];
+            uint32_t d = (key >> shift) & (R - 1);
+            uint32_t g = s_run[d] + (j - s_dstart[d]);
+            kout[g] = key;
+            vout[g] = s_vals[j];
+        }
+        __syncthreads();
+        for (int d = tid; d < R; d += SORT_THREADS) s_run[d] += s_tot[d];
+        __syncthreads();
+    }
+}
+
+int sort_grid_blocks() {
+    static int g = 0;
+    if (!g) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        g = sms * 2;
+    }
+    return g;
+}
+
+int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n_host, const uint32_t* n_dev, int bits, SortScratch& sc,
+                     int grid, cudaStream_t st, cudaError_t* err) {
+    *err = cudaSuccess;
+    if (bits <= 0) return 0;
+    size_t cap = n_host;
+    if ((*err = sc.keys2.ensure(cap * 4 + 16)) != cudaSuccess) return 0;
+    if ((*err = sc.vals2.ensure(cap * 4 + 16)) != cudaSuccess) return 0;
+    if ((*err = sc.hist.ensure((size_t)grid * 512 * 4)) != cudaSuccess) return 0;
+    uint32_t* k[2] = {keys, sc.keys2.as<uint32_t>()};
+    uint32_t* v[2] = {vals, sc.vals2.as<uint32_t>()};
+    int cur = 0;
+    int shift = 0;
+    // 8-bit digits; a final pass over fewer significant bits still reads 8
+    // (the bits above `bits` are zero in every key, so they do not reorder).
+    while (shift < bits) {
+        uint32_t* hist = sc.hist.as<uint32_t>();
+        k_upsweep<8><<<grid, SORT_THREADS, 0, st>>>(k[cur], n_dev, n_host, shift, hist);
+        k_scan_hist<8><<<1, SORT_THREADS, 0, st>>>(hist, grid);
+        k_downsweep<8><<<grid, SORT_THREADS, 0, st>>>(k[cur], v[cur], k[cur ^ 1], v[cur ^ 1], n_dev, n_host, shift, hist);
+        cur ^= 1;
+        shift += 8;
+    }
+    *err = cudaGetLastError();
+    return cur;
+}
+
+}  // namespace rgs

@@ -1,0 +1,285 @@
+"""CUDA path vs the CPU oracle, through the C ABI, on seeded scenes.
+
+Bars (stated per test): projection, tile lists and the forward caches are
+compared bit for bit (the kernels evaluate the reference's arithmetic in the
+same order); images must stay within 1e-4 max abs; blend accumulators and
+parameter gradients within 1e-3 relative (atomic summation order differs);
+Adam, densification and opacity reset bit for bit.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import rgsplat_b200 as R
+from rgsplat_b200 import debug as D
+from rgsplat_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+IMG_TOL = 1e-4
+GRAD_TOL = 1e-3
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    return R.Context()
+
+
+def small_scene(n=4000, seed=1, w=256, h=256, fx=300.0, dist=4.0, log_scale=(-4.0, 0.5), opacity=(0.0, 1.0)):
+    g = scenes.random_gaussians(n, seed, 1.0, log_scale, opacity)
+    cam = scenes.look_at((0.3, -0.2, -dist), (0.0, 0.0, 0.0), w, h, fx)
+    tgt_g = scenes.perturbed(g, seed + 100)
+    rgb, _, _ = O.render_color(tgt_g, cam)
+    target = np.concatenate([rgb, np.ones((h, w, 1), np.float32)], axis=2)
+    return g, cam, target
+
+
+def group_rel_err(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    den = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / den) if den > 0 else float(np.linalg.norm(a - b))
+
+
+GROUPS = {"position": slice(0, 3), "rotation": slice(3, 7), "log_scale": slice(7, 10), "opacity": slice(10, 11),
+          "sh": slice(11, 59), "screen": slice(59, 60)}
+
+
+def assert_grads_close(g_gpu, g_ref, tol=GRAD_TOL):
+    for name, sl in GROUPS.items():
+        e = group_rel_err(g_gpu[:, sl], g_ref[:, sl])
+        assert e < tol, f"{name}: relative error {e:.3e}"
+
+
+# ---- projection / binning (bit exact) -----------------------------------------
+@pytest.mark.parametrize("seed", [1, 2])
+def test_projection_bit_exact(ctx, seed):
+    g, cam, _ = small_scene(seed=seed)
+    vis, rec, rect = D.project(g, cam, ctx)
+    ovis, orec, orect = O.project(g, cam)
+    assert np.array_equal(vis, ovis)
+    m = vis.astype(bool)
+    assert np.array_equal(rect[m], orect[m])
+    # rec10 = sx, sy, conic3, color3, opacity, depth; oracle rec16 = sx, sy, conic3, cov3, color3, raw3, opacity, depth
+    ref = np.concatenate([orec[:, 0:5], orec[:, 8:11], orec[:, 14:16]], axis=1)
+    assert np.array_equal(rec[m].view(np.uint32), ref[m].view(np.uint32))
+
+
+@pytest.mark.parametrize("seed", [1, 3])
+def test_tile_lists_bit_exact(ctx, seed):
+    g, cam, _ = small_scene(seed=seed)
+    offs, ent = D.tile_lists(g, cam, ctx)
+    ooffs, oent = O.tile_lists(g, cam)
+    assert np.array_equal(offs, ooffs)
+    assert np.array_equal(ent, oent)
+
+
+def test_tile_lists_depth_ties_break_by_index(ctx):
+    # identical Gaussians: equal depth bits, so the order must be the index order
+    g, cam, _ = small_scene(n=50, seed=4)
+    g[10:20] = g[10]
+    offs, ent = D.tile_lists(g, cam, ctx)
+    ooffs, oent = O.tile_lists(g, cam)
+    assert np.array_equal(ent, oent)
+
+
+# ---- forward (bit exact, image tolerance 1e-4) --------------------------------
+@pytest.mark.parametrize("bg", [(0.0, 0.0, 0.0), (0.2, 0.5, 0.9)])
+def test_forward_matches_oracle(ctx, bg):
+    g, cam, _ = small_scene(seed=5)
+    rgb, ft, last = D.forward(g, cam, bg, ctx)
+    orgb, oft, olast = O.render_color(g, cam, bg)
+    assert np.abs(rgb - orgb).max() <= IMG_TOL
+    assert np.array_equal(last, olast)
+    assert np.array_equal(rgb.view(np.uint32), orgb.view(np.uint32)), f"max diff {np.abs(rgb - orgb).max()}"
+    assert np.array_equal(ft.view(np.uint32), oft.view(np.uint32))
+
+
+def test_render_color_odd_sizes(ctx):
+    g, cam, _ = small_scene(n=3000, seed=6, w=173, h=91, fx=200.0)
+    rgb = R.render_color(g, cam, (0.1, 0.1, 0.1), ctx=ctx)
+    orgb, _, _ = O.render_color(g, cam, (0.1, 0.1, 0.1))
+    assert np.abs(rgb - orgb).max() <= IMG_TOL
+
+
+# ---- loss ------------------------------------------------------------------------
+def test_photometric_loss_grad_matches_oracle(ctx):
+    rng = np.random.default_rng(7)
+    w, h = 77, 53
+    rendered = rng.uniform(0, 1, (h, w, 3)).astype(np.float32)
+    target = np.concatenate([rng.uniform(0, 1, (h, w, 3)), np.ones((h, w, 1))], axis=2).astype(np.float32)
+    loss, dl = R.photometric_loss_grad(rendered, target, w, h, 0.2, ctx=ctx)
+    oloss, odl = O.photometric_loss_grad(rendered, target, w, h, 0.2)
+    assert abs(loss - oloss) <= 1e-4 * abs(oloss)
+    assert np.abs(dl - odl).max() <= 1e-9 + 1e-5 * np.abs(odl).max()
+
+
+def test_image_loss_gradient_matches_finite_difference_gpu(ctx):
+    """src/cpu/backward.rs:858-892 through the CUDA loss kernel."""
+    from tests import refcases
+
+    w, h = 12, 12
+    rendered, target = refcases.loss_grad_images(w, h)
+    _, grad = R.photometric_loss_grad(rendered, target, w, h, 0.2, ctx=ctx)
+    eps = np.float32(1e-3)
+    for (p, ch) in [(0, 0), (40, 1), (77, 2), (143, 0)]:
+        idx = p * 3 + ch
+        rp, rm = rendered.copy(), rendered.copy()
+        rp[idx] += eps
+        rm[idx] -= eps
+        lp = R.photometric_loss_grad(rp, target, w, h, 0.2, ctx=ctx)[0]
+        lm = R.photometric_loss_grad(rm, target, w, h, 0.2, ctx=ctx)[0]
+        num = (np.float32(lp) - np.float32(lm)) / (2 * eps)
+        assert abs(grad[idx] - num) < 2e-3
+
+
+def test_ssim_of_identical_images_is_one_gpu(ctx):
+    """src/cpu/backward.rs:849-856: identical images give loss (1 - lambda) * 0 + lambda * (1 - 1)."""
+    w = h = 16
+    img = np.array([(i % 7) / 7.0 for i in range(w * h)], np.float32)
+    rendered = np.repeat(img[:, None], 3, axis=1)
+    target = np.concatenate([rendered, np.ones((w * h, 1), np.float32)], axis=1)
+    loss, _ = R.photometric_loss_grad(rendered, target, w, h, 1.0, ctx=ctx)
+    assert abs(loss) < 1e-4
+
+
+# ---- backward -----------------------------------------------------------------------
+def test_blend_backward_accumulators(ctx):
+    g, cam, target = small_scene(seed=8)
+    acc, dl = D.backward(g, cam, target, (0.0, 0.0, 0.0), 0.2, ctx)
+    ref = O.render_and_backward(g, cam, target, (0.0, 0.0, 0.0), 0.2)
+    assert np.abs(dl - ref.dl_dpix).max() <= 1e-9 + 1e-5 * np.abs(ref.dl_dpix).max()
+    for k in range(9):
+        e = group_rel_err(acc[:, k], ref.acc[:, k])
+        assert e < GRAD_TOL, f"accumulator {k}: {e:.3e}"
+
+
+@pytest.mark.parametrize("lam,bg", [(0.2, (0.0, 0.0, 0.0)), (0.0, (0.3, 0.3, 0.3))])
+def test_render_and_backward_matches_oracle(ctx, lam, bg):
+    g, cam, target = small_scene(seed=9)
+    loss, grads = R.render_and_backward(g, cam, target, bg, R.LossConfig(lam), ctx=ctx)
+    ref = O.render_and_backward(g, cam, target, bg, lam)
+    assert abs(loss - ref.loss) <= 1e-4 * abs(ref.loss)
+    assert_grads_close(grads, ref.grads)
+
+
+def test_parameter_gradients_match_finite_difference_gpu(ctx):
+    """src/cpu/backward.rs:906-982 through the C ABI: analytic vs central differences."""
+    from tests import refcases as RC
+
+    cam = O.identity_camera(24, 24)
+    target = RC.solid_target(24, 24, [0.0, 0.0, 0.0])
+    g0 = RC.fd_scene()
+    cfg = R.LossConfig(0.0)
+    _, grads = R.render_and_backward(g0, cam, target, (0, 0, 0), cfg, ctx=ctx)
+    grad = grads[0]
+    eps = np.float32(1e-3)
+
+    def numeric(idx):
+        gp, gm = g0.copy(), g0.copy()
+        gp[0, idx] += eps
+        gm[0, idx] -= eps
+        lp = R.render_and_backward(gp, cam, target, (0, 0, 0), cfg, ctx=ctx)[0]
+        lm = R.render_and_backward(gm, cam, target, (0, 0, 0), cfg, ctx=ctx)[0]
+        return (lp - lm) / (2 * float(eps))
+
+    def check(a, n, name):
+        rel = abs(a - n) / max(abs(a), abs(n), 1e-4)
+        assert rel < 0.05 or abs(a - n) < 3e-4, f"{name}: {a} vs {n}"
+
+    for k in range(3):
+        check(grad[k], numeric(k), "d_position")
+    check(grad[10], numeric(3), "d_opacity")
+    for k in range(3):
+        check(grad[7 + k], numeric(8 + k), "d_log_scale")
+    for k in [0, 1, 16, 33]:
+        check(grad[11 + k], numeric(11 + k), "d_sh")
+    q = g0[0, 4:8].astype(np.float64)
+    num_rot = np.array([numeric(4 + k) for k in range(4)])
+    proj = lambda v: np.asarray(v, np.float64) - np.dot(v, q) * q  # noqa: E731
+    a, nn = proj(grad[3:7]), proj(num_rot)
+    assert np.linalg.norm(a - nn) / max(np.linalg.norm(nn), 1e-3) < 0.1
+
+
+def test_render_produces_nonblack_for_visible_gaussian_gpu(ctx):
+    """src/cpu/backward.rs:894-904."""
+    from tests import refcases as RC
+
+    cam = O.identity_camera(32, 32)
+    g = RC.gaussian_new([0.0, 0.0, 2.0])
+    g[3] = RC.logit(0.9)
+    g[8:11] = -1.5
+    g[11] = 2.0
+    img = R.render_color(g[None], cam, ctx=ctx)
+    assert img[16, 16, 0] > 0.01
+
+
+# ---- optimizer (bit exact) -------------------------------------------------------
+def test_adam_step_matches_oracle(ctx):
+    g, cam, target = small_scene(n=2000, seed=10)
+    _, grads = R.render_and_backward(g, cam, target, ctx=ctx)
+    cfg = R.TrainConfig()
+    ga, go = g.copy(), g.copy()
+    sa, so = R.AdamState(g.shape[0]), O.AdamState(g.shape[0])
+    for _ in range(3):
+        R.adam_step(ga, grads, sa, cfg, ctx=ctx)
+        O.adam_step(go, grads, so, O.TrainConfig())
+    assert sa.t == so.t == 3
+    assert np.array_equal(ga.view(np.uint32), go.view(np.uint32))
+    assert np.array_equal(sa.m1.view(np.uint32), so.m1.view(np.uint32))
+    assert np.array_equal(sa.m2.view(np.uint32), so.m2.view(np.uint32))
+    assert np.array_equal(sa.grad_accum, so.grad_accum)
+    assert np.array_equal(sa.grad_denom, so.grad_denom)
+
+
+def test_densify_and_prune_matches_oracle(ctx):
+    g = scenes.random_gaussians(5000, 11, 1.0, (-3.0, 1.0), (0.0, 2.0))
+    rng = np.random.default_rng(11)
+    st_r, st_o = R.AdamState(g.shape[0]), O.AdamState(g.shape[0])
+    acc = rng.exponential(3e-4, g.shape[0]).astype(np.float32)
+    den = rng.integers(0, 4, g.shape[0]).astype(np.uint32)
+    for st in (st_r, st_o):
+        st.grad_accum[:] = acc
+        st.grad_denom[:] = den
+    for max_g in (3_000_000, 5200):
+        cfg = R.TrainConfig(max_gaussians=max_g)
+        ocfg = O.TrainConfig(max_gaussians=max_g)
+        extent = R.estimate_scene_extent(g)
+        assert extent == O.estimate_scene_extent(g)
+        a = st_r.grad_accum.copy(), st_r.grad_denom.copy()
+        out_r = R.densify_and_prune(g, st_r, cfg, extent, ctx=ctx)
+        out_o = O.densify_and_prune(g, st_o, ocfg, extent)
+        assert out_r.shape == out_o.shape
+        assert np.array_equal(out_r.view(np.uint32), out_o.view(np.uint32))
+        for st in (st_r, st_o):
+            st.grad_accum[: a[0].shape[0]] = a[0]
+            st.grad_denom[: a[1].shape[0]] = a[1]
+
+
+def test_reset_opacities_matches_oracle(ctx):
+    g = scenes.random_gaussians(3000, 12, 1.0, (-4.0, 0.5), (0.0, 3.0))
+    gr, go = g.copy(), g.copy()
+    R.reset_opacities(gr, ctx=ctx)
+    O.reset_opacities(go)
+    assert np.array_equal(gr.view(np.uint32), go.view(np.uint32))
+
+
+def test_training_reduces_photometric_loss_gpu(ctx):
+    """tests/training_reduces_loss.rs:38-84 on the CUDA path."""
+    from tests import refcases as RC
+
+    w = h = 32
+    cam = O.identity_camera(w, h)
+    target = RC.solid_target(w, h, [0.2, 0.55, 0.5])
+    gs = RC.training_scene()
+    cfg = R.TrainConfig()
+    adam = R.AdamState(gs.shape[0])
+    initial, _ = R.render_and_backward(gs, cam, target, ctx=ctx)
+    last = initial
+    for _ in range(200):
+        last, grads = R.render_and_backward(gs, cam, target, ctx=ctx)
+        R.adam_step(gs, grads, adam, cfg, ctx=ctx)
+    assert last < initial * 0.5
+    img = R.render_color(gs, cam, ctx=ctx)
+    for ch in range(3):
+        assert abs(img[h // 2, w // 2, ch] - target[0, 0, ch]) < 0.15
