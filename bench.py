@@ -1,0 +1,454 @@
+#!/usr/bin/env python
+"""Benchmark: train iter/s (fwd + bwd + Adam) of the 1M-Gaussian, 8-views-per-step
+workload (batched multi-view step vs the plain per-view path), on B200.
+
+Workload (synthetic, seeded; no dataset is involved): 1M Gaussians with means
+U[-2, 2]^3, log-scales N(-4, 0.5), normalised N(0, 1) quaternions, opacity
+logits N(0, 1), SH degree 3 (DC N(0, 0.3), rest N(0, 0.05)); 128 cameras on a
+radius-5 Fibonacci sphere cycling through 1600x1064, 1280x720 and 960x540
+(fx = fy = 1.25 * width); 8 views per step picked with the reference's
+xorshift64 camera shuffle (src/pipeline/mod.rs:224-230); targets rendered from
+the scene with means perturbed by N(0, 0.02).
+
+`python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]`
+prints one JSON line (rank 0). Under torchrun (N > 1) every rank trains its own
+8 views per step and the gradients are summed with an NCCL all-reduce before a
+replicated Adam step (view-parallel data parallelism, weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "train iter/s (fwd+bwd+Adam) batched vs plain GPU path, 1M Gaussians, at tol"
+UNIT = "iter/s"
+WORKLOAD = "1M Gaussians, SH3, 8 views/step from 128 sphere cameras {1600x1064, 1280x720, 960x540}"
+
+
+def xorshift_views(state: list, n_cams: int, k: int) -> list[int]:
+    """src/pipeline/mod.rs:224-230: x ^= x << 13; x ^= x >> 7; x ^= x << 17; x % n."""
+    out = []
+    m = (1 << 64) - 1
+    for _ in range(k):
+        x = state[0]
+        x ^= (x << 13) & m
+        x ^= x >> 7
+        x ^= (x << 17) & m
+        state[0] = x
+        out.append(x % n_cams)
+    return out
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--scale", type=float, default=1.0, help="fraction of the 1M Gaussians (smaller cases for profiling)")
+    p.add_argument("--views", type=int, default=8)
+    p.add_argument("--plain-steps", type=int, default=None)
+    p.add_argument("--cpu-seconds", type=float, default=25.0, help="CPU-baseline sample budget")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--tile", default="16x16")
+    p.add_argument("--batch", type=int, default=256)
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{device}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                                          "-i", str(self.device)], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def build_workload(scale: float):
+    from rgsplat_b200 import scenes
+
+    cfg = scenes.config(3, n=max(1000, int(round(1_000_000 * scale))))
+    g = scenes.make_gaussians(cfg)
+    return cfg, g
+
+
+def render_targets(R, scenes, cfg, g, ctx):
+    """RGBA targets of every camera, rendered on the GPU from the perturbed scene."""
+    tr = R.Trainer(scenes.perturbed(g, cfg.seed + 1), cfg.cameras, ctx=ctx)
+    targets = []
+    for i, c in enumerate(cfg.cameras):
+        rgb = tr.render(i)
+        t = np.empty((c.height, c.width, 4), np.float32)
+        t[..., :3] = rgb
+        t[..., 3] = 1.0
+        targets.append(t)
+    return targets
+
+
+def algorithmic_bytes(stage: str, n: int, views: int, pairs: int, pixels: int) -> float:
+    """Per-step algorithmic HBM bytes of a stage (what an ideal kernel must move)."""
+    if stage == "project":
+        return views * n * 60.0 * 4 + views * n * (48 + 12)          # params read per view; record + count + key written
+    if stage == "depth_sort":
+        return views * n * 8.0 * 2                                    # (key, slot) read + written once
+    if stage == "emit":
+        return views * n * 8.0 + pairs * 8.0                          # counts + order read; pairs written
+    if stage == "tile_sort":
+        return pairs * 8.0 * 2                                        # (tile, slot) read + written once
+    if stage == "ranges":
+        return pairs * 4.0 + 0.0
+    if stage == "forward":
+        return pairs * (4.0 + 48.0) + pixels * 20.0                   # slot + record per pair; rgb, T, last written
+    if stage == "loss":
+        return pixels * (12.0 + 16.0 + 12.0)                          # rendered, target read; dL/dpix written
+    if stage == "backward":
+        return pixels * 20.0 + pairs * (4.0 + 48.0) + views * n * 48.0  # caches + records read; accumulators
+    if stage == "geometry_adam":
+        return n * 240.0 * 3 * 2 + views * n * (48.0 + 4.0)            # params, m1, m2 read + written; accumulators
+    return 0.0
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the oracle (C++ restatement of the reference CPU path) on host cores
+# ---------------------------------------------------------------------------
+def cpu_sample(g, cfg, targets_fn, budget_s: float, max_samples: int):
+    """Times render_and_backward of single views plus one Adam step on the host
+    cores; returns (seconds per 8-view iteration, samples, threads)."""
+    import oracle as O
+
+    threads = O.set_threads(os.cpu_count() or 1)
+    st = [0x9E3779B97F4A7C15]
+    view_times = []
+    t_start = time.perf_counter()
+    gg = np.ascontiguousarray(g)
+    state = O.AdamState(g.shape[0])
+    last_grads = None
+    while len(view_times) < max_samples and (time.perf_counter() - t_start) < budget_s:
+        v = xorshift_views(st, len(cfg.cameras), 1)[0]
+        cam = cfg.cameras[v]
+        tgt = targets_fn(v)
+        t0 = time.perf_counter()
+        out = O.render_and_backward(gg, cam, tgt, (0.0, 0.0, 0.0), 0.2)
+        view_times.append(time.perf_counter() - t0)
+        last_grads = out.grads
+    t0 = time.perf_counter()
+    O.adam_step(gg, last_grads, state, O.TrainConfig())
+    adam_s = time.perf_counter() - t0
+    per_view = float(np.mean(view_times))
+    return 8 * per_view + adam_s, len(view_times), threads, per_view, adam_s
+
+
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return
+    import oracle as O
+    from rgsplat_b200 import scenes
+
+    cfg, g = build_workload(args.scale)
+    tg = scenes.perturbed(g, cfg.seed + 1)
+    cache = {}
+
+    def target(v):
+        if v not in cache:
+            rgb, _, _ = O.render_color(tg, cfg.cameras[v])
+            cache[v] = np.concatenate([rgb, np.ones((cfg.cameras[v].height, cfg.cameras[v].width, 1), np.float32)], axis=2)
+        return cache[v]
+
+    O.set_threads(os.cpu_count() or 1)
+    budget = max(60.0, 12.0 * max(args.steps, 1))
+    s_per_iter, samples, threads, per_view, adam_s = cpu_sample(g, cfg, target, budget, max(args.steps, 1))
+    value = 1.0 / s_per_iter
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": samples,
+        "warmup": 0, "ms_per_step": s_per_iter * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_gaussians": int(g.shape[0]), "views_per_step": 8},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{samples} single-view render_and_backward calls ({per_view:.2f} s each) + one "
+                                   f"Adam step ({adam_s:.2f} s) of the full workload; iter = 8 views + Adam"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+class _CudaArray:
+    """Zero-copy torch view of a device buffer owned by the library."""
+
+    def __init__(self, ptr: int, nbytes: int):
+        self.__cuda_array_interface__ = {"shape": (nbytes // 4,), "typestr": "<f4", "data": (ptr, False), "version": 3, "strides": None}
+
+
+def run_ours(args, rank: int, world: int, local_rank: int):
+    import torch
+
+    import rgsplat_b200 as R
+    from rgsplat_b200 import scenes
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local_rank))
+
+    tw, th = (int(x) for x in args.tile.split("x"))
+    ctx = R.Context(device=local_rank, tile=(tw, th), batch=args.batch)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    cfg, g = build_workload(args.scale)
+    n = g.shape[0]
+    V = args.views
+    with torch.cuda.stream(stream):
+        targets = render_targets(R, scenes, cfg, g, ctx)
+        trainer = R.Trainer(g, cfg.cameras, targets, ctx=ctx)
+    tcfg = R.TrainConfig()
+    lcfg = R.LossConfig(0.2)
+    rng_state = [0x9E3779B97F4A7C15 ^ (rank * 0x5851F42D4C957F2D)]
+    schedule = [xorshift_views(rng_state, len(cfg.cameras), V) for _ in range(args.warmup + 3 * args.steps + 8)]
+    it = iter(schedule)
+
+    def step_batched():
+        views = next(it)
+        if world == 1:
+            return trainer.step(views, mode=R.Trainer.BATCHED, loss_cfg=lcfg, train_cfg=tcfg)
+        losses = trainer.backward(views, loss_cfg=lcfg, mode=R.Trainer.BATCHED)
+        ptr, nbytes, _ = trainer.grad_buffer()
+        grad = torch.as_tensor(_CudaArray(ptr, nbytes), device=f"cuda:{local_rank}")
+        dist.all_reduce(grad)
+        trainer.apply_adam(tcfg, denom_increment=V * world)
+        return losses
+
+    def step_plain():
+        views = next(it)
+        if world == 1:
+            return trainer.step(views, mode=R.Trainer.PLAIN, loss_cfg=lcfg, train_cfg=tcfg)
+        losses = trainer.backward(views, loss_cfg=lcfg, mode=R.Trainer.PLAIN)
+        ptr, nbytes, _ = trainer.grad_buffer()
+        grad = torch.as_tensor(_CudaArray(ptr, nbytes), device=f"cuda:{local_rank}")
+        dist.all_reduce(grad)
+        trainer.apply_adam(tcfg, denom_increment=V * world)
+        return losses
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def timed(fn, k: int) -> float:
+        """Seconds for k steps: CUDA events on the library's stream, max over ranks."""
+        barrier()
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(k):
+                fn()
+            e1.record(stream)
+        e1.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        if dist is not None:
+            tt = torch.tensor([t], device=f"cuda:{local_rank}")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return t
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step_batched()
+        ctx.set_profiling(True)
+        ctx.stage_times(reset=True)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    t_batched = timed(step_batched, args.steps)
+    clock_info = clocks.stop()
+    stage_ms = ctx.stage_times(reset=True)
+    pairs_last = ctx.stats()["pairs"]
+    ctx.set_profiling(False)
+
+    kp = args.plain_steps if args.plain_steps is not None else max(3, args.steps // 2)
+    with torch.cuda.stream(stream):
+        step_plain()
+    t_plain = timed(step_plain, kp)
+
+    # e2e: the step's inputs (8 RGBA targets + cameras) copied from pinned host
+    # memory through the C ABI every step, losses read back.
+    e2e = None
+    if not args.no_e2e:
+        pinned = {}
+
+        def pinned_target(v):
+            if v not in pinned:
+                t = torch.from_numpy(targets[v]).pin_memory()
+                pinned[v] = t
+            return pinned[v]
+
+        h2d = [0]
+
+        def step_e2e():
+            views = schedule[-1 - (step_e2e.k % 8)]
+            step_e2e.k += 1
+            b = 0
+            for v in views:
+                t = pinned_target(v)
+                trainer.set_target_ptr(v, t.data_ptr())
+                b += t.numel() * 4
+            h2d[0] = b + len(views) * 100
+            return trainer.step(views, mode=R.Trainer.BATCHED, loss_cfg=lcfg, train_cfg=tcfg)
+
+        step_e2e.k = 0
+        for v in set(x for vs in schedule[-8:] for x in vs):
+            pinned_target(v)
+        with torch.cuda.stream(stream):
+            step_e2e()
+        ke = max(3, args.steps // 2)
+        t_e2e = timed(step_e2e, ke)
+        e2e = {"value": world * ke / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d[0]), "d2h_bytes_per_step": 4 * V + 8}
+
+    value = world * args.steps / t_batched
+    plain_value = world * kp / t_plain
+    ms_per_step = t_batched / args.steps * 1e3
+
+    # roofline of the dominant stage
+    pixels_per_step = int(np.mean([sum(cfg.cameras[v].width * cfg.cameras[v].height for v in vs) for vs in schedule[: args.steps]]))
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs")
+    peak_src = "measured"
+    if not hbm:
+        hbm, peak_src = 6650.0, "fallback"
+    per_step_ms = {k: v / args.steps for k, v in stage_ms.items()}
+    dom = max(per_step_ms, key=per_step_ms.get) if per_step_ms else None
+    roofline = None
+    stages = {}
+    for k, ms in per_step_ms.items():
+        b = algorithmic_bytes(k, n, V, pairs_last, pixels_per_step)
+        gbs = b / (ms / 1e3) / 1e9 if ms > 0 else 0.0
+        stages[k] = {"ms": round(ms, 4), "algorithmic_gb": round(b / 1e9, 4), "achieved_gbs": round(gbs, 1), "frac_hbm": round(gbs / hbm, 4)}
+    if dom:
+        b = algorithmic_bytes(dom, n, V, pairs_last, pixels_per_step)
+        ach = b / (per_step_ms[dom] / 1e3) / 1e9
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                    "frac": round(ach / hbm, 4), "peak_source": peak_src, "traffic": None}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            import oracle as O
+
+            tg = scenes.perturbed(g, cfg.seed + 1)
+            s_iter, samples, threads, per_view, adam_s = cpu_sample(g, cfg, lambda v: targets[v], args.cpu_seconds, 4)
+            cpu = {"value": 1.0 / s_iter, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"{samples} single-view render_and_backward calls ({per_view:.2f} s each) + one Adam step "
+                             f"({adam_s:.2f} s) of this workload on the oracle; iter = 8 views + Adam"}
+            del tg
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms_per_step, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_gaussians": n, "views_per_step": V, "parallelism": f"view-dp{world}",
+                       "mode": "batched (graph-captured, one launch per stage)", "tile": args.tile, "batch": args.batch,
+                       "l2": "inputs larger than L2 (236 MB params + 480 MB moments + targets)",
+                       "plain_iter_per_s": round(plain_value, 4), "batched_over_plain": round(value / plain_value, 3),
+                       "pairs_per_step": int(pairs_last), "pixels_per_step": pixels_per_step},
+            "e2e": e2e,
+            "gpu_launches": None,
+            "roofline": roofline,
+            "stages": stages,
+            "cpu_baseline": cpu,
+            "clocks": clock_info,
+        }
+        # kernels launched per batched step: project 1, depth sort 4x3, count
+        # scan 2, emit 1, tile sort 3 per 8 bits, ranges 1, forward 1, loss 2,
+        # backward 1, geometry+Adam 1 (+ memsets)
+        tile_bits = max(1, int(np.ceil(np.log2(max(2, V * max(-(-c.width // tw) * -(-c.height // th) for c in cfg.cameras))))))
+        per_step = 1 + 12 + 2 + 1 + 3 * ((tile_bits + 7) // 8) + 1 + 1 + 2 + 1 + 1
+        line["gpu_launches"] = per_step * args.steps
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -180,10 +180,11 @@ int rgs_trainer_step(rgs_ctx* ctx, const uint32_t* views, size_t nviews, const f
                      const rgs_loss_config* loss_cfg, const rgs_train_config* train_cfg, int mode,
                      float* losses_out);
 
-/* Render + backward only: gradients (summed over views) stay on the device
- * for rgs_trainer_get_grads / rgs_trainer_grad_buffer / rgs_trainer_apply_adam. */
+/* Render + backward only (mode as for rgs_trainer_step): gradients summed over
+ * the views stay on the device for rgs_trainer_get_grads /
+ * rgs_trainer_grad_buffer / rgs_trainer_apply_adam. */
 int rgs_trainer_backward(rgs_ctx* ctx, const uint32_t* views, size_t nviews, const float bg[3],
-                         const rgs_loss_config* loss_cfg, float* losses_out);
+                         const rgs_loss_config* loss_cfg, int mode, float* losses_out);
 int rgs_trainer_get_grads(rgs_ctx* ctx, float* out /* n * 60 */);
 /* Device gradient buffer (15 float4 planes of `plane_stride` Gaussians) for a
  * collective (e.g. an NCCL all-reduce across view-parallel ranks). */
@@ -196,6 +197,25 @@ int rgs_trainer_densify_and_prune(rgs_ctx* ctx, const rgs_train_config* cfg, flo
 int rgs_trainer_reset_opacities(rgs_ctx* ctx);
 int rgs_trainer_get_adam_state(rgs_ctx* ctx, rgs_adam_state* state); /* fills caller arrays (len >= count) */
 int rgs_trainer_set_adam_state(rgs_ctx* ctx, const rgs_adam_state* state);
+
+/* Issue all work on `cuda_stream` (a cudaStream_t that is not the legacy
+ * default stream), or on the context's own stream when NULL. */
+int rgs_set_stream(rgs_ctx* ctx, void* cuda_stream);
+
+/* Per-stage device timing of trainer steps (CUDA events between stages). */
+#define RGS_NUM_STAGES 9
+#define RGS_STAGE_PROJECT 0
+#define RGS_STAGE_DEPTH_SORT 1
+#define RGS_STAGE_EMIT 2
+#define RGS_STAGE_TILE_SORT 3
+#define RGS_STAGE_RANGES 4
+#define RGS_STAGE_FORWARD 5
+#define RGS_STAGE_LOSS 6
+#define RGS_STAGE_BACKWARD 7
+#define RGS_STAGE_GEOMETRY_ADAM 8
+int rgs_set_profiling(rgs_ctx* ctx, int on);
+/* Milliseconds per stage accumulated since the last reset (reset != 0 clears). */
+int rgs_get_stage_times(rgs_ctx* ctx, float* ms_out /* RGS_NUM_STAGES */, int reset);
 
 /* Statistics of the last step or render. */
 typedef struct rgs_stats {

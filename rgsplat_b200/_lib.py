@@ -23,6 +23,8 @@ RGS_ERR_NO_DEVICE = -7
 
 RGS_STEP_PLAIN = 0
 RGS_STEP_BATCHED = 1
+RGS_NUM_STAGES = 9
+STAGE_NAMES = ("project", "depth_sort", "emit", "tile_sort", "ranges", "forward", "loss", "backward", "geometry_adam")
 RGS_PROJECT_WGSL = 0
 RGS_PROJECT_CPU_MATH = 1
 
@@ -139,7 +141,7 @@ SIGNATURES = {
     "rgs_trainer_set_cameras": (C.c_int, [CTX, C.POINTER(rgs_camera), C.c_size_t]),
     "rgs_trainer_set_target": (C.c_int, [CTX, C.c_size_t, FP]),
     "rgs_trainer_step": (C.c_int, [CTX, U32P, C.c_size_t, FP, C.POINTER(rgs_loss_config), C.POINTER(rgs_train_config), C.c_int, FP]),
-    "rgs_trainer_backward": (C.c_int, [CTX, U32P, C.c_size_t, FP, C.POINTER(rgs_loss_config), FP]),
+    "rgs_trainer_backward": (C.c_int, [CTX, U32P, C.c_size_t, FP, C.POINTER(rgs_loss_config), C.c_int, FP]),
     "rgs_trainer_get_grads": (C.c_int, [CTX, FP]),
     "rgs_trainer_grad_buffer": (C.c_int, [CTX, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     "rgs_trainer_apply_adam": (C.c_int, [CTX, C.POINTER(rgs_train_config), C.c_uint32]),
@@ -149,6 +151,9 @@ SIGNATURES = {
     "rgs_trainer_get_adam_state": (C.c_int, [CTX, C.POINTER(rgs_adam_state)]),
     "rgs_trainer_set_adam_state": (C.c_int, [CTX, C.POINTER(rgs_adam_state)]),
     "rgs_get_stats": (C.c_int, [CTX, C.POINTER(rgs_stats)]),
+    "rgs_set_stream": (C.c_int, [CTX, C.c_void_p]),
+    "rgs_set_profiling": (C.c_int, [CTX, C.c_int]),
+    "rgs_get_stage_times": (C.c_int, [CTX, FP, C.c_int]),
     # include/rgsplat_debug.h
     "rgs_debug_project": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), C.POINTER(C.c_int32), FP, C.POINTER(C.c_int32)]),
     "rgs_debug_tile_lists": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), C.POINTER(C.c_uint64), C.POINTER(C.c_int32),

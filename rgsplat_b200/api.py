@@ -172,6 +172,19 @@ class Context:
         except Exception:
             pass
 
+    def set_stream(self, cuda_stream: int | None) -> None:
+        """Issue work on an external cudaStream_t (not the legacy default stream)."""
+        self.check(self.lib.rgs_set_stream(self.handle, C.c_void_p(cuda_stream or None)))
+
+    def set_profiling(self, on: bool) -> None:
+        self.check(self.lib.rgs_set_profiling(self.handle, 1 if on else 0))
+
+    def stage_times(self, reset: bool = False) -> dict:
+        """Milliseconds per training-step stage accumulated since the last reset."""
+        ms = (C.c_float * L.RGS_NUM_STAGES)()
+        self.check(self.lib.rgs_get_stage_times(self.handle, ms, 1 if reset else 0))
+        return {n: float(ms[i]) for i, n in enumerate(L.STAGE_NAMES)}
+
     def stats(self) -> dict:
         s = L.rgs_stats()
         self.check(self.lib.rgs_get_stats(self.handle, C.byref(s)))
@@ -368,6 +381,10 @@ class Trainer:
             raise ValueError("target must be w*h*4 RGBA floats")
         self.ctx.check(self.lib.rgs_trainer_set_target(self.ctx.handle, index, _fp(t)))
 
+    def set_target_ptr(self, index: int, host_ptr: int) -> None:
+        """Upload camera ``index``'s RGBA target from a raw host pointer (e.g. pinned memory)."""
+        self.ctx.check(self.lib.rgs_trainer_set_target(self.ctx.handle, index, C.cast(C.c_void_p(host_ptr), L.FP)))
+
     def __len__(self) -> int:
         n = C.c_size_t(0)
         self.ctx.check(self.lib.rgs_trainer_count(self.ctx.handle, C.byref(n)))
@@ -390,11 +407,13 @@ class Trainer:
                                                  C.byref(tc), int(mode), _fp(losses)))
         return losses[: v.size]
 
-    def backward(self, views: Sequence[int], bg=(0.0, 0.0, 0.0), loss_cfg: LossConfig | None = None) -> np.ndarray:
+    def backward(self, views: Sequence[int], bg=(0.0, 0.0, 0.0), loss_cfg: LossConfig | None = None,
+                 mode: int = L.RGS_STEP_PLAIN) -> np.ndarray:
         v = np.ascontiguousarray(views, dtype=np.uint32)
         losses = np.zeros(max(v.size, 1), np.float32)
         lc = (loss_cfg or LossConfig()).to_c()
-        self.ctx.check(self.lib.rgs_trainer_backward(self.ctx.handle, v.ctypes.data_as(L.U32P), v.size, _fp(_f32(bg)), C.byref(lc), _fp(losses)))
+        self.ctx.check(self.lib.rgs_trainer_backward(self.ctx.handle, v.ctypes.data_as(L.U32P), v.size, _fp(_f32(bg)), C.byref(lc),
+                                                     int(mode), _fp(losses)))
         return losses[: v.size]
 
     def grads(self) -> np.ndarray:

@@ -70,6 +70,8 @@ __global__ void __launch_bounds__(TW * TH) k_blend_fwd(BlendArgs a) {
         float T = 1.0f, C0 = 0.0f, C1 = 0.0f, C2 = 0.0f;
         int last = -1;
         bool done = !inside;
+        // whether the pixel's reference tile list is non-empty
+        bool seen = !RECT && rg.y > rg.x;
         for (uint32_t b0 = rg.x; b0 < rg.y; b0 += BATCH) {
             if (__syncthreads_count(!done) == 0) break;
             for (int j = tid; j < BATCH; j += NT) {
@@ -86,7 +88,10 @@ __global__ void __launch_bounds__(TW * TH) k_blend_fwd(BlendArgs a) {
             for (int j = 0; j < nb && !done; ++j) {
                 const float4 A = s_a[j];
                 const float4 Q = s_c[j];
-                if (RECT && !in_rect(Q.w, s_k[j].w, px, py)) continue;
+                if (RECT) {
+                    if (!in_rect(Q.w, s_k[j].w, px, py)) continue;
+                    seen = true;
+                }
                 const float dx = pxf - A.x, dy = pyf - A.y;
                 const float power = -0.5f * (Q.x * dx * dx + 2.0f * Q.y * dx * dy + Q.z * dy * dy);
                 if (power > 0.0f || power < RGS_POWER_CUT) continue;
@@ -105,9 +110,12 @@ __global__ void __launch_bounds__(TW * TH) k_blend_fwd(BlendArgs a) {
         }
         if (inside) {
             size_t pix = (size_t)c.pix_base + (size_t)py * c.width + px;
-            a.rgb[pix * 3 + 0] = C0 + T * a.bg[0];
-            a.rgb[pix * 3 + 1] = C1 + T * a.bg[1];
-            a.rgb[pix * 3 + 2] = C2 + T * a.bg[2];
+            // forward_pass skips tiles whose list is empty, leaving their pixels
+            // at 0 rather than bg (src/cpu/backward.rs:313-315, 124)
+            const bool black = a.empty_tile_black && !seen;
+            a.rgb[pix * 3 + 0] = black ? 0.0f : C0 + T * a.bg[0];
+            a.rgb[pix * 3 + 1] = black ? 0.0f : C1 + T * a.bg[1];
+            a.rgb[pix * 3 + 2] = black ? 0.0f : C2 + T * a.bg[2];
             a.final_t[pix] = T;
             a.last[pix] = last;
         }

@@ -84,6 +84,13 @@ struct rgs_ctx {
     cudaGraphExec_t gexec = nullptr;
     std::vector<uint64_t> g_key;
     rgs_stats stats{};
+    cudaStream_t own_stream = nullptr;
+    // per-stage timing (boundaries 0..RGS_NUM_STAGES)
+    bool prof = false;
+    cudaEvent_t ev[RGS_NUM_STAGES + 1] = {};
+    bool ev_marked[RGS_NUM_STAGES + 1] = {};
+    bool graph_marked[RGS_NUM_STAGES + 1] = {};
+    float stage_ms[RGS_NUM_STAGES] = {};
 };
 
 namespace {
@@ -104,6 +111,28 @@ int cuda_fail(rgs_ctx* c, cudaError_t e, const char* what) {
         cudaError_t e_ = (call);                             \
         if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
     } while (0)
+
+// Stage boundary i (0 = start, RGS_NUM_STAGES = end) of the step being issued.
+void mark(rgs_ctx* ctx, int i) {
+    if (!ctx->prof) return;
+    cudaEventRecord(ctx->ev[i], ctx->st);
+    ctx->ev_marked[i] = true;
+}
+
+// After the stream has drained: add the elapsed time of every stage whose two
+// boundaries were recorded.
+void prof_collect(rgs_ctx* ctx) {
+    if (!ctx->prof) return;
+    for (int i = 0; i < RGS_NUM_STAGES; ++i) {
+        int j = i + 1;
+        while (j <= RGS_NUM_STAGES && !ctx->ev_marked[j]) ++j;
+        if (!ctx->ev_marked[i] || j > RGS_NUM_STAGES) continue;
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, ctx->ev[i], ctx->ev[j]) == cudaSuccess) ctx->stage_ms[i] += ms;
+    }
+    cudaGetLastError();
+    for (int i = 0; i <= RGS_NUM_STAGES; ++i) ctx->ev_marked[i] = false;
+}
 
 // General 4x4 inverse by cofactors, in double (Camera::view_matrix inverts c2w,
 // src/math/mod.rs:155-160).
@@ -336,16 +365,20 @@ struct Binned {
 
 // Projection + depth sort + pair emission + tile sort + ranges for one batch.
 // `k_host` >= 0 means the pair count was read back (plain path).
-int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tiles, bool host_count, Binned& out) {
+int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tiles, bool host_count, Binned& out,
+              bool project = true) {
     cudaStream_t st = ctx->st;
     const size_t S = (size_t)s.n * V;
     uint32_t* sc = ctx->scalars.as<uint32_t>();
-    launch_project(s.params.as<float4>(), s.n, s.cap, cams_dev, V, ctx->opt.tile_w, ctx->opt.tile_h, ctx->rec.as<float4>(),
-                   ctx->cnt.as<uint32_t>(), ctx->dkey.as<uint32_t>(), ctx->ids.as<uint32_t>(), st);
+    if (project)
+        launch_project(s.params.as<float4>(), s.n, s.cap, cams_dev, V, ctx->opt.tile_w, ctx->opt.tile_h,
+                       ctx->rec.as<float4>(), ctx->cnt.as<uint32_t>(), ctx->dkey.as<uint32_t>(), ctx->ids.as<uint32_t>(), st);
+    mark(ctx, 1);
     cudaError_t e;
     int which = radix_sort_pairs(ctx->dkey.as<uint32_t>(), ctx->ids.as<uint32_t>(), (uint32_t)S, nullptr, 32, ctx->sort,
                                  ctx->sort_grid, st, &e);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "depth sort");
+    mark(ctx, 2);
     const uint32_t* order = which ? ctx->sort.vals2.as<uint32_t>() : ctx->ids.as<uint32_t>();
     launch_count_scan(order, ctx->cnt.as<uint32_t>(), (uint32_t)S, ctx->block_sums.as<uint32_t>(), sc + SC_PAIRS,
                       ctx->sort_grid, st);
@@ -380,13 +413,16 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
                       cams_dev, V, (uint32_t)s.n, ctx->opt.tile_w, ctx->opt.tile_h, ctx->pkeys.as<uint32_t>(),
                       ctx->pvals.as<uint32_t>(), ctx->pair_cap, (int*)(sc + SC_OVERFLOW), sc + SC_PAIRS, sc + SC_PAIRS_EFF,
                       ctx->sort_grid, st);
+    mark(ctx, 3);
     int which2 = radix_sort_pairs(ctx->pkeys.as<uint32_t>(), ctx->pvals.as<uint32_t>(), ctx->pair_cap, sc + SC_PAIRS_EFF,
                                   bits_for(std::max<size_t>(tiles, 2)), ctx->sort, ctx->sort_grid, st, &e);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "tile sort");
+    mark(ctx, 4);
     out.keys = which2 ? ctx->sort.keys2.as<uint32_t>() : ctx->pkeys.as<uint32_t>();
     out.vals = which2 ? ctx->sort.vals2.as<uint32_t>() : ctx->pvals.as<uint32_t>();
     CK(cudaMemsetAsync(ctx->ranges.p, 0, std::max<size_t>(tiles, 1) * sizeof(uint2), st));
     launch_tile_ranges(out.keys, sc + SC_PAIRS, ctx->pair_cap, ctx->ranges.as<uint2>(), st);
+    mark(ctx, 5);
     CK(cudaGetLastError());
     return RGS_OK;
 }
@@ -410,6 +446,7 @@ BlendArgs blend_args(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, cons
     a.acc = ctx->acc.as<float4>();
     a.work = ctx->scalars.as<uint32_t>() + (fwd ? SC_WORK_F : SC_WORK_B);
     a.rect_filter = 0;
+    a.empty_tile_black = 1;
     return a;
 }
 
@@ -439,10 +476,12 @@ int run_view_plain(rgs_ctx* ctx, Scene& s, const DevCam& dc_in, const float* tar
     if (rc) return rc;
     DevCam* cams_dev;
     if ((rc = upload_single_cam(ctx, dc, &cams_dev))) return rc;
+    mark(ctx, 0);
     Binned b;
     if ((rc = bin_batch(ctx, s, cams_dev, 1, tiles, true, b))) return rc;
     BlendArgs fa = blend_args(ctx, s, cams_dev, 1, nullptr, tiles, b, bg, true);
     launch_blend_forward(fa, ctx->opt.tile_w, ctx->opt.tile_h, ctx->opt.batch, st);
+    mark(ctx, 6);
     CK(cudaGetLastError());
     if (rgb_host) {
         CK(cudaMemcpyAsync(rgb_host, ctx->rgb.p, px * 3 * 4, cudaMemcpyDeviceToHost, st));
@@ -452,15 +491,19 @@ int run_view_plain(rgs_ctx* ctx, Scene& s, const DevCam& dc_in, const float* tar
     float* losses_dev = (float*)((char*)ctx->outd.p + offsetof(StepOut, losses));
     launch_loss(cams_dev, 1, (int)lb, ctx->rgb.as<float>(), lambda, ctx->dl.as<float>(), ctx->partials.as<float>(), losses_dev,
                 nullptr, st);
+    mark(ctx, 7);
     CK(cudaMemsetAsync(ctx->acc.p, 0, std::max<size_t>(s.n, 1) * 3 * sizeof(float4), st));
     BlendArgs ba = blend_args(ctx, s, cams_dev, 1, nullptr, tiles, b, bg, false);
     launch_blend_backward(ba, ctx->opt.tile_w, ctx->opt.tile_h, ctx->opt.batch, st);
+    mark(ctx, 8);
     launch_geometry(s.params.as<float4>(), s.n, s.cap, cams_dev, 1, ctx->cnt.as<uint32_t>(), ctx->acc.as<float4>(),
                     s.grads.as<float4>(), accumulate ? 1 : 0, st);
+    mark(ctx, 9);
     CK(cudaGetLastError());
     if (loss_out) {
         CK(cudaMemcpyAsync(loss_out, losses_dev, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        prof_collect(ctx);
     }
     return RGS_OK;
 }
@@ -535,7 +578,8 @@ int rgs_create(const rgs_options* opts, rgs_ctx** out) {
     ctx->device = o.device;
     cudaError_t e = cudaSetDevice(o.device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, o.device);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
+    ctx->st = ctx->own_stream;
     if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->hdr_h, sizeof(StepHdr));
     if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->out_h, sizeof(StepOut));
     if (e != cudaSuccess) {
@@ -568,7 +612,9 @@ void rgs_destroy(rgs_ctx* ctx) {
     for (DBuf* b : bufs) b->release();
     if (ctx->hdr_h) cudaFreeHost(ctx->hdr_h);
     if (ctx->out_h) cudaFreeHost(ctx->out_h);
-    if (ctx->st) cudaStreamDestroy(ctx->st);
+    for (int i = 0; i <= RGS_NUM_STAGES; ++i)
+        if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
 }
 
@@ -578,6 +624,32 @@ int rgs_synchronize(rgs_ctx* ctx) {
     int rc = check_ctx(ctx);
     if (rc) return rc;
     CK(cudaStreamSynchronize(ctx->st));
+    return RGS_OK;
+}
+
+int rgs_set_stream(rgs_ctx* ctx, void* cuda_stream) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->st = cuda_stream ? (cudaStream_t)cuda_stream : ctx->own_stream;
+    return RGS_OK;
+}
+
+int rgs_set_profiling(rgs_ctx* ctx, int on) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (on && !ctx->ev[0])
+        for (int i = 0; i <= RGS_NUM_STAGES; ++i) CK(cudaEventCreate(&ctx->ev[i]));
+    ctx->prof = on != 0;
+    return RGS_OK;
+}
+
+int rgs_get_stage_times(rgs_ctx* ctx, float* ms_out, int reset) {
+    if (!ctx) return RGS_ERR_INVALID_ARG;
+    if (ms_out)
+        for (int i = 0; i < RGS_NUM_STAGES; ++i) ms_out[i] = ctx->stage_ms[i];
+    if (reset)
+        for (int i = 0; i < RGS_NUM_STAGES; ++i) ctx->stage_ms[i] = 0.0f;
     return RGS_OK;
 }
 
@@ -780,8 +852,36 @@ int rgs_project(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera
 
 int rgs_gpu_render(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, int mode, const float bg[3],
                    float* rgb_out) {
-    (void)gaussians; (void)n; (void)camera; (void)mode; (void)bg; (void)rgb_out;
-    return fail(ctx, RGS_ERR_INVALID_ARG, "rgs_gpu_render: not available in this build");
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!camera || !bg || !rgb_out || (n && !gaussians)) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
+    if (mode != RGS_PROJECT_WGSL && mode != RGS_PROJECT_CPU_MATH) return fail(ctx, RGS_ERR_INVALID_ARG, "unknown mode");
+    DevCam dc;
+    if ((rc = make_devcam(ctx, *camera, dc))) return rc;
+    Scene& s = ctx->sc;
+    if ((rc = upload_gaussians(ctx, s, gaussians, n))) return rc;
+    size_t px, tiles, lb;
+    assign_bases(&dc, 1, px, tiles, lb);
+    if ((rc = ensure_work(ctx, std::max<size_t>(n, 1), px, tiles, lb, 1))) return rc;
+    DevCam* cams_dev;
+    if ((rc = upload_single_cam(ctx, dc, &cams_dev))) return rc;
+    CK(ctx->stage_b.ensure(std::max<size_t>(n, 1) * 40));
+    CK(ctx->stage_c.ensure(std::max<size_t>(n, 1) * 4));
+    launch_project_wgsl(s.params.as<float4>(), (int)n, s.cap, cams_dev, mode == RGS_PROJECT_CPU_MATH ? 1 : 0,
+                        ctx->stage_b.as<float>(), ctx->stage_c.as<uint32_t>(), ctx->st);
+    launch_composite_prepare(ctx->stage_b.as<float>(), (int)n, cams_dev, ctx->opt.tile_w, ctx->opt.tile_h,
+                             ctx->rec.as<float4>(), ctx->cnt.as<uint32_t>(), ctx->dkey.as<uint32_t>(), ctx->ids.as<uint32_t>(),
+                             ctx->st);
+    Binned b;
+    if ((rc = bin_batch(ctx, s, cams_dev, 1, tiles, true, b, false))) return rc;
+    BlendArgs fa = blend_args(ctx, s, cams_dev, 1, nullptr, tiles, b, bg, true);
+    fa.rect_filter = 1;
+    fa.empty_tile_black = 0;
+    launch_blend_forward(fa, ctx->opt.tile_w, ctx->opt.tile_h, ctx->opt.batch, ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(rgb_out, ctx->rgb.p, px * 12, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return RGS_OK;
 }
 
 // ===========================================================================
@@ -909,7 +1009,8 @@ void batch_caps(rgs_ctx* ctx, int V, size_t& px, size_t& tiles, size_t& lb) {
     lb = ml * V;
 }
 
-int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], float lambda, const rgs_train_config& tc) {
+int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], float lambda, const rgs_train_config& tc,
+                    bool fused) {
     Scene& s = ctx->tr;
     cudaStream_t st = ctx->st;
     if (ctx->gexec) {
@@ -927,22 +1028,32 @@ int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], fl
     uint32_t* sc = ctx->scalars.as<uint32_t>();
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     cudaMemcpyAsync(ctx->hdr.p, ctx->hdr_h, sizeof(StepHdr), cudaMemcpyHostToDevice, st);
+    mark(ctx, 0);
     Binned b;
     int rc = bin_batch(ctx, s, cams_dev, V, tiles_cap, false, b);
     if (!rc) {
         BlendArgs fa = blend_args(ctx, s, cams_dev, V, &hd->total_tiles, tiles_cap, b, bg, true);
         launch_blend_forward(fa, ctx->opt.tile_w, ctx->opt.tile_h, ctx->opt.batch, st);
+        mark(ctx, 6);
         launch_loss(cams_dev, V, 0, ctx->rgb.as<float>(), lambda, ctx->dl.as<float>(), ctx->partials.as<float>(), losses_dev,
                     &hd->total_loss_blocks, st);
+        mark(ctx, 7);
         cudaMemsetAsync(ctx->acc.p, 0, std::max<size_t>(S, 1) * 3 * sizeof(float4), st);
         BlendArgs ba = blend_args(ctx, s, cams_dev, V, &hd->total_tiles, tiles_cap, b, bg, false);
         launch_blend_backward(ba, ctx->opt.tile_w, ctx->opt.tile_h, ctx->opt.batch, st);
-        AdamArgs a;
-        adam_args(ctx, s, tc, a);
-        a.denom_inc = (uint32_t)V;
-        a.skip_flag = (const int*)(sc + SC_OVERFLOW);
-        a.bc_dev = hd->bc;
-        launch_geometry_adam(cams_dev, V, s.n, s.cap, ctx->cnt.as<uint32_t>(), ctx->acc.as<float4>(), a, st);
+        mark(ctx, 8);
+        if (fused) {
+            AdamArgs a;
+            adam_args(ctx, s, tc, a);
+            a.denom_inc = (uint32_t)V;
+            a.skip_flag = (const int*)(sc + SC_OVERFLOW);
+            a.bc_dev = hd->bc;
+            launch_geometry_adam(cams_dev, V, s.n, s.cap, ctx->cnt.as<uint32_t>(), ctx->acc.as<float4>(), a, st);
+        } else {
+            launch_geometry(s.params.as<float4>(), s.n, s.cap, cams_dev, V, ctx->cnt.as<uint32_t>(), ctx->acc.as<float4>(),
+                            s.grads.as<float4>(), 0, st);
+        }
+        mark(ctx, 9);
         cudaMemcpyAsync(&ctx->out_h->pairs, sc + SC_PAIRS, 4, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(&ctx->out_h->overflow, sc + SC_OVERFLOW, 4, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(ctx->out_h->losses, losses_dev, sizeof(float) * V, cudaMemcpyDeviceToHost, st);
@@ -964,7 +1075,7 @@ int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], fl
 // Batched path: one launch per stage over all views, replayed from a CUDA
 // graph; the fused geometry-backward + Adam kernel ends the step.
 int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], float lambda, const rgs_train_config& tc,
-                 float* losses) {
+                 float* losses, bool fused) {
     Scene& s = ctx->tr;
     StepHdr* h = ctx->hdr_h;
     for (int v = 0; v < V; ++v) {
@@ -983,52 +1094,56 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
     if (rc) return rc;
     if (!ctx->pkeys.p && (rc = ensure_pairs(ctx, S * 4))) return rc;
     if ((rc = ensure_moments(ctx, s, s.n))) return rc;
+    const uint64_t tstep = fused ? 1 : 0;
     for (int attempt = 0; attempt < 4; ++attempt) {
-        s.t += 1;
+        s.t += tstep;
         h->bc[0] = 1.0f - powi_f(tc.beta1, (int)s.t);
         h->bc[1] = 1.0f - powi_f(tc.beta2, (int)s.t);
         // Everything a captured graph bakes in: sizes, every buffer address, and
         // the loss weight, background and optimiser constants.
-        std::vector<uint64_t> key = {(uint64_t)s.n, (uint64_t)s.cap, (uint64_t)V, (uint64_t)s.mcap, ctx->pair_cap, px_cap,
-                                     tiles_cap, lb_cap};
-        const DBuf* bufs[] = {&s.params, &s.m1, &s.m2, &s.accum, &s.denom, &ctx->rec, &ctx->cnt, &ctx->dkey, &ctx->ids,
-                              &ctx->acc, &ctx->pkeys, &ctx->pvals, &ctx->ranges, &ctx->rgb, &ctx->final_t, &ctx->last,
-                              &ctx->dl, &ctx->partials, &ctx->scalars, &ctx->block_sums, &ctx->hdr, &ctx->outd,
+        const DBuf* bufs[] = {&s.params, &s.grads, &s.m1, &s.m2, &s.accum, &s.denom, &ctx->rec, &ctx->cnt, &ctx->dkey,
+                              &ctx->ids, &ctx->acc, &ctx->pkeys, &ctx->pvals, &ctx->ranges, &ctx->rgb, &ctx->final_t,
+                              &ctx->last, &ctx->dl, &ctx->partials, &ctx->scalars, &ctx->block_sums, &ctx->hdr, &ctx->outd,
                               &ctx->sort.hist, &ctx->sort.keys2, &ctx->sort.vals2};
-        for (const DBuf* b : bufs) key.push_back((uint64_t)(uintptr_t)b->p);
         float fk[14] = {bg[0], bg[1], bg[2], lambda, tc.lr_position, tc.lr_rotation, tc.lr_scale, tc.lr_opacity,
                         tc.lr_sh_dc, tc.lr_sh_rest, tc.beta1, tc.beta2, tc.eps, (float)ctx->opt.reference_compat};
-        for (float f : fk) {
-            uint32_t u;
-            std::memcpy(&u, &f, 4);
-            key.push_back(u);
-        }
-        if (!ctx->gexec || key != ctx->g_key) {
-            if ((rc = capture_batched(ctx, V, tiles_cap, bg, lambda, tc))) {
-                s.t -= 1;
-                return rc;
-            }
-            // capture may have grown scratch buffers: recompute the key
-            key.resize(8);
+        auto make_key = [&]() {
+            std::vector<uint64_t> key = {(uint64_t)s.n, (uint64_t)s.cap, (uint64_t)V, (uint64_t)s.mcap, ctx->pair_cap,
+                                         px_cap, tiles_cap, lb_cap, (uint64_t)fused, (uint64_t)ctx->prof,
+                                         (uint64_t)(uintptr_t)ctx->st};
             for (const DBuf* b : bufs) key.push_back((uint64_t)(uintptr_t)b->p);
             for (float f : fk) {
                 uint32_t u;
                 std::memcpy(&u, &f, 4);
                 key.push_back(u);
             }
-            ctx->g_key = key;
+            return key;
+        };
+        std::vector<uint64_t> key = make_key();
+        if (!ctx->gexec || key != ctx->g_key) {
+            for (int i = 0; i <= RGS_NUM_STAGES; ++i) ctx->ev_marked[i] = false;
+            if ((rc = capture_batched(ctx, V, tiles_cap, bg, lambda, tc, fused))) {
+                s.t -= tstep;
+                return rc;
+            }
+            for (int i = 0; i <= RGS_NUM_STAGES; ++i) ctx->graph_marked[i] = ctx->ev_marked[i];
+            ctx->g_key = make_key();  // capture may have grown scratch buffers
         }
         CK(cudaGraphLaunch(ctx->gexec, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
+        if (ctx->prof) {
+            for (int i = 0; i <= RGS_NUM_STAGES; ++i) ctx->ev_marked[i] = ctx->graph_marked[i];
+            prof_collect(ctx);
+        }
         ctx->stats.pairs = ctx->out_h->pairs;
         if (!ctx->out_h->overflow) {
             if (losses)
                 for (int v = 0; v < V; ++v) losses[v] = ctx->out_h->losses[v];
-            s.mlen = std::max(s.mlen, s.n);
+            if (fused) s.mlen = std::max(s.mlen, s.n);
             return RGS_OK;
         }
         // pair buffer too small: Adam was skipped on the device; grow and redo
-        s.t -= 1;
+        s.t -= tstep;
         ctx->stats.overflow_retries += 1;
         if ((rc = ensure_pairs(ctx, ctx->out_h->pairs))) return rc;
     }
@@ -1045,7 +1160,8 @@ int rgs_trainer_step(rgs_ctx* ctx, const uint32_t* views, size_t nviews, const f
     if (rc) return rc;
     if (!bg || !loss_cfg || !train_cfg) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
     if ((rc = check_views(ctx, views, nviews, true))) return rc;
-    if (mode == RGS_STEP_BATCHED) return batched_step(ctx, views, (int)nviews, bg, loss_cfg->lambda_dssim, *train_cfg, losses_out);
+    if (mode == RGS_STEP_BATCHED)
+        return batched_step(ctx, views, (int)nviews, bg, loss_cfg->lambda_dssim, *train_cfg, losses_out, true);
     if (mode != RGS_STEP_PLAIN) return fail(ctx, RGS_ERR_INVALID_ARG, "unknown step mode");
     if ((rc = ensure_moments(ctx, ctx->tr, ctx->tr.n))) return rc;
     if ((rc = plain_backward(ctx, views, nviews, bg, loss_cfg->lambda_dssim, losses_out))) return rc;
@@ -1055,11 +1171,17 @@ int rgs_trainer_step(rgs_ctx* ctx, const uint32_t* views, size_t nviews, const f
 }
 
 int rgs_trainer_backward(rgs_ctx* ctx, const uint32_t* views, size_t nviews, const float bg[3], const rgs_loss_config* loss_cfg,
-                         float* losses_out) {
+                         int mode, float* losses_out) {
     int rc = check_ctx(ctx);
     if (rc) return rc;
     if (!bg || !loss_cfg) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
     if ((rc = check_views(ctx, views, nviews, true))) return rc;
+    if (mode == RGS_STEP_BATCHED) {
+        rgs_train_config tc;
+        rgs_train_config_default(&tc);
+        return batched_step(ctx, views, (int)nviews, bg, loss_cfg->lambda_dssim, tc, losses_out, false);
+    }
+    if (mode != RGS_STEP_PLAIN) return fail(ctx, RGS_ERR_INVALID_ARG, "unknown step mode");
     return plain_backward(ctx, views, nviews, bg, loss_cfg->lambda_dssim, losses_out);
 }
 

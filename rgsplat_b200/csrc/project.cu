@@ -235,4 +235,49 @@ void launch_project_wgsl(const float4* params, int n, int cap, const DevCam* cam
     k_project_wgsl<<<(n + 255) / 256, 256, 0, st>>>(params, n, cap, cam, cpu_math, splats10, keys);
 }
 
+// GpuRenderer::render's CPU compositor (src/gpu/compute.rs:243-296, with
+// depth_order of src/gpu/sort.rs:10-17) expressed as splat records for the
+// tile pipeline: a splat is drawn iff alpha >= 1/255 and depth > 0, over the
+// pixel box floor(s - r) .. ceil(s + r) with r = 3 / sqrt(lambda_min(conic)).
+// The blend kernel then tests each pixel against that box (RECT mode).
+__global__ void __launch_bounds__(256) k_composite_prepare(const float* __restrict__ sp, int n, const DevCam* __restrict__ cam,
+                                                           int tile_w, int tile_h, float4* __restrict__ rec,
+                                                           uint32_t* __restrict__ cnt, uint32_t* __restrict__ dkey,
+                                                           uint32_t* __restrict__ ids) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    ids[i] = (uint32_t)i;
+    const float* s = sp + (size_t)i * 10;
+    const int w = cam->width, h = cam->height;
+    cnt[i] = 0;
+    dkey[i] = 0xFFFFFFFFu;
+    if (!(s[8] >= 1.0f / 255.0f && s[9] > 0.0f)) return;
+    float a = s[2], b = s[3], c = s[4];
+    float mid = 0.5f * (a + c);
+    float disc = sqrtf(0.25f * (a - c) * (a - c) + b * b);
+    float lmin = fmaxf(mid - disc, 1e-6f);
+    float rad = 3.0f * sqrtf(1.0f / lmin);
+    // Rust `as usize` / `as i64` saturate and map NaN to 0
+    float fx0 = fmaxf(floorf(s[0] - rad), 0.0f), fy0 = fmaxf(floorf(s[1] - rad), 0.0f);
+    float fx1 = ceilf(s[0] + rad), fy1 = ceilf(s[1] + rad);
+    int x0 = fx0 != fx0 ? 0 : (fx0 >= (float)w ? w : (int)fx0);
+    int y0 = fy0 != fy0 ? 0 : (fy0 >= (float)h ? h : (int)fy0);
+    int x1 = fx1 != fx1 ? 0 : (fx1 <= 0.0f ? 0 : (fx1 >= (float)w ? w : (int)fx1));
+    int y1 = fy1 != fy1 ? 0 : (fy1 <= 0.0f ? 0 : (fy1 >= (float)h ? h : (int)fy1));
+    if (x0 >= x1 || y0 >= y1) return;
+    int ctx0 = x0 / tile_w, cty0 = y0 / tile_h;
+    int ctx1 = (x1 + tile_w - 1) / tile_w, cty1 = (y1 + tile_h - 1) / tile_h;
+    rec[i] = make_float4(s[0], s[1], s[8], s[9]);
+    rec[(size_t)n + i] = make_float4(a, b, c, __uint_as_float((uint32_t)x0 | ((uint32_t)x1 << 16)));
+    rec[2 * (size_t)n + i] = make_float4(s[5], s[6], s[7], __uint_as_float((uint32_t)y0 | ((uint32_t)y1 << 16)));
+    cnt[i] = (uint32_t)((ctx1 - ctx0) * (cty1 - cty0));
+    dkey[i] = __float_as_uint(s[9]);
+}
+
+void launch_composite_prepare(const float* splats10, int n, const DevCam* cam, int tile_w, int tile_h, float4* rec,
+                              uint32_t* cnt, uint32_t* dkey, uint32_t* ids, cudaStream_t st) {
+    if (n <= 0) return;
+    k_composite_prepare<<<(n + 255) / 256, 256, 0, st>>>(splats10, n, cam, tile_w, tile_h, rec, cnt, dkey, ids);
+}
+
 }  // namespace rgs

@@ -119,6 +119,8 @@ void launch_project(const float4* params, int n, int cap, const DevCam* cams, in
                     cudaStream_t st);
 void launch_project_wgsl(const float4* params, int n, int cap, const DevCam* cam, int cpu_math,
                          float* splats10, uint32_t* keys, cudaStream_t st);
+void launch_composite_prepare(const float* splats10, int n, const DevCam* cam, int tile_w, int tile_h,
+                              float4* rec, uint32_t* cnt, uint32_t* dkey, uint32_t* ids, cudaStream_t st);
 
 // sort.cu: stable LSD radix sort of (key, value) u32 pairs on bits [0, bits).
 // n_dev may be null (then n_host is used). Returns which buffer holds the
@@ -155,6 +157,7 @@ struct BlendArgs {
     float4* acc;
     uint32_t* work;                // dynamic tile counter (zeroed by the launcher)
     int rect_filter;               // per-pixel reference-tile membership test
+    int empty_tile_black;          // pixels of empty reference tiles render 0, not bg
 };
 void launch_blend_forward(const BlendArgs& a, int tile_w, int tile_h, int batch, cudaStream_t st);
 void launch_blend_backward(const BlendArgs& a, int tile_w, int tile_h, int batch, cudaStream_t st);

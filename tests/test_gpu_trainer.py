@@ -1,0 +1,271 @@
+"""Device-resident trainer (plain and batched steps), tile shapes, edge cases and
+the GpuRenderer drop-in, against the CPU oracle."""
+import numpy as np
+import pytest
+
+import oracle as O
+import rgsplat_b200 as R
+from rgsplat_b200 import debug as D
+from rgsplat_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+IMG_TOL = 1e-4
+
+
+def multi_view_scene(n=3000, seed=21, sizes=((160, 120), (128, 96), (96, 64)), ncams=6, log_scale=(-3.5, 0.5)):
+    g = scenes.random_gaussians(n, seed, 1.0, log_scale, (0.0, 1.0))
+    cams = scenes.sphere_cameras(ncams, 4.0, list(sizes), 1.2)
+    tg = scenes.perturbed(g, seed + 1)
+    targets = []
+    for c in cams:
+        rgb, _, _ = O.render_color(tg, c)
+        targets.append(np.concatenate([rgb, np.ones((c.height, c.width, 1), np.float32)], axis=2))
+    return g, cams, targets
+
+
+def oracle_step(g, cams, targets, views, state, cfg, lam=0.2, bg=(0.0, 0.0, 0.0)):
+    """Multi-view semantics: summed per-view gradients, one Adam step, denom += V."""
+    total = None
+    losses = []
+    for v in views:
+        out = O.render_and_backward(g, cams[v], targets[v], bg, lam)
+        losses.append(out.loss)
+        total = out.grads.copy() if total is None else total + out.grads
+    O.adam_step(g, total, state, cfg)
+    state.grad_denom += np.uint32(len(views) - 1)
+    return np.array(losses, np.float32), total
+
+
+def test_trainer_plain_step_matches_oracle():
+    g, cams, targets = multi_view_scene()
+    tr = R.Trainer(g, cams, targets)
+    views = [0, 3]
+    losses = tr.step(views, mode=R.Trainer.PLAIN)
+    go = g.copy()
+    so = O.AdamState(g.shape[0])
+    olosses, _ = oracle_step(go, cams, targets, views, so, O.TrainConfig())
+    assert np.allclose(losses, olosses, rtol=1e-4)
+    gt = tr.gaussians()
+    assert np.abs(gt - go).max() < 1e-6
+    st = tr.adam_state()
+    assert st.t == 1
+    assert np.array_equal(st.grad_denom[: g.shape[0]], so.grad_denom)
+    assert np.allclose(st.grad_accum[: g.shape[0]], so.grad_accum, rtol=1e-3, atol=1e-9)
+
+
+def test_trainer_backward_grads_match_oracle_sum():
+    g, cams, targets = multi_view_scene(seed=22)
+    tr = R.Trainer(g, cams, targets)
+    tr.backward([1, 2, 5])
+    grads = tr.grads()
+    ref = sum(O.render_and_backward(g, cams[v], targets[v]).grads for v in (1, 2, 5))
+    for sl in (slice(0, 3), slice(3, 7), slice(7, 10), slice(10, 11), slice(11, 59), slice(59, 60)):
+        e = np.linalg.norm(grads[:, sl] - ref[:, sl]) / np.linalg.norm(ref[:, sl])
+        assert e < 1e-3
+
+
+def test_batched_step_matches_plain_over_several_steps():
+    g, cams, targets = multi_view_scene(seed=23)
+    tp = R.Trainer(g, cams, targets)
+    tb = R.Trainer(g, cams, targets)
+    steps = [[0, 1, 2], [3, 4, 5], [1, 4, 0], [2, 2, 3]]
+    for vs in steps:
+        lp = tp.step(vs, mode=R.Trainer.PLAIN)
+        lb = tb.step(vs, mode=R.Trainer.BATCHED)
+        assert np.allclose(lp, lb, rtol=1e-4, atol=1e-7)
+    a, b = tp.gaussians(), tb.gaussians()
+    assert np.abs(a - b).max() < 1e-5
+    sa, sb = tp.adam_state(), tb.adam_state()
+    assert sa.t == sb.t == len(steps)
+    assert np.array_equal(sa.grad_denom, sb.grad_denom)
+    assert tb.ctx.stats()["graph_captures"] >= 1
+
+
+def test_batched_pair_overflow_recovers():
+    # large footprints: far more (Gaussian, tile) pairs than the initial capacity
+    g, cams, targets = multi_view_scene(n=400, seed=24, log_scale=(-1.0, 0.3))
+    tp = R.Trainer(g, cams, targets)
+    tb = R.Trainer(g, cams, targets)
+    lp = tp.step([0, 1], mode=R.Trainer.PLAIN)
+    lb = tb.step([0, 1], mode=R.Trainer.BATCHED)
+    assert np.allclose(lp, lb, rtol=1e-4)
+    assert tb.ctx.stats()["overflow_retries"] >= 1
+    assert np.abs(tp.gaussians() - tb.gaussians()).max() < 1e-5
+    assert tb.adam_state().t == 1
+
+
+@pytest.mark.parametrize("tile", [(8, 32), (32, 8)])
+@pytest.mark.parametrize("batch", [128, 512])
+def test_tile_shapes_keep_reference_semantics(tile, batch):
+    g, cam_list, targets = multi_view_scene(n=3000, seed=25, sizes=((150, 110),), ncams=1)
+    cam, target = cam_list[0], targets[0]
+    ctx = R.Context(tile=tile, batch=batch)
+    rgb, ft, _ = D.forward(g, cam, (0.2, 0.1, 0.0), ctx)
+    orgb, oft, _ = O.render_color(g, cam, (0.2, 0.1, 0.0))
+    assert np.array_equal(rgb.view(np.uint32), orgb.view(np.uint32)), f"max diff {np.abs(rgb - orgb).max()}"
+    assert np.array_equal(ft.view(np.uint32), oft.view(np.uint32))
+    loss, grads = R.render_and_backward(g, cam, target, ctx=ctx)
+    ref = O.render_and_backward(g, cam, target)
+    assert abs(loss - ref.loss) <= 1e-4 * ref.loss
+    e = np.linalg.norm(grads - ref.grads) / np.linalg.norm(ref.grads)
+    assert e < 1e-3
+
+
+def test_trainer_densify_matches_oracle():
+    g, cams, targets = multi_view_scene(n=2000, seed=26)
+    tr = R.Trainer(g, cams, targets)
+    for vs in ([0, 1], [2, 3]):
+        tr.step(vs, mode=R.Trainer.PLAIN)
+    st = tr.adam_state()
+    gt = tr.gaussians()
+    cfg = R.TrainConfig(densify_grad_threshold=float(np.quantile(st.grad_accum / np.maximum(st.grad_denom, 1), 0.7)))
+    extent = R.estimate_scene_extent(g)
+    so = O.AdamState(gt.shape[0])
+    so.grad_accum[:] = st.grad_accum[: gt.shape[0]]
+    so.grad_denom[:] = st.grad_denom[: gt.shape[0]]
+    ocfg = O.TrainConfig(densify_grad_threshold=cfg.densify_grad_threshold)
+    expect = O.densify_and_prune(gt, so, ocfg, extent)
+    n_new = tr.densify_and_prune(cfg, extent)
+    assert n_new == expect.shape[0]
+    assert np.array_equal(tr.gaussians().view(np.uint32), expect.view(np.uint32))
+    st2 = tr.adam_state()
+    assert not st2.grad_accum.any() and not st2.grad_denom.any()
+    # moments keep their slots (AdamState::resize never compacts, optimizer.rs:97-105)
+    assert np.array_equal(st2.m1[: st.m1.shape[0]], st.m1[: st2.m1.shape[0]][: st.m1.shape[0]])
+    tr.step([4, 5], mode=R.Trainer.BATCHED)
+
+
+# ---- edge cases -------------------------------------------------------------------
+def test_empty_scene_renders_black_and_has_loss():
+    cam = scenes.look_at((0.0, 0.0, -4.0), (0.0, 0.0, 0.0), 64, 48, 80.0)
+    g = np.zeros((0, 59), np.float32)
+    rgb = R.render_color(g, cam, (0.5, 0.5, 0.5))
+    assert not rgb.any()
+    target = np.ones((48, 64, 4), np.float32)
+    loss, grads = R.render_and_backward(g, cam, target)
+    oloss = O.render_and_backward(g, cam, target).loss
+    assert grads.shape == (0, 60)
+    assert abs(loss - oloss) <= 1e-5
+
+
+def test_all_behind_camera():
+    g = scenes.random_gaussians(500, 27, 1.0, (-4.0, 0.5), (0.0, 1.0))
+    g[:, 2] = np.abs(g[:, 2]) + 10.0  # camera at z=-4 looks +z... move all behind by flipping the camera
+    cam = scenes.look_at((0.0, 0.0, 5.0), (0.0, 0.0, 20.0), 64, 64, 80.0)
+    rgb = R.render_color(g, cam)
+    orgb, _, _ = O.render_color(g, cam)
+    assert np.array_equal(rgb, orgb)
+
+
+def test_huge_gaussian_covers_image():
+    g = scenes.random_gaussians(20, 28, 0.2, (0.5, 0.1), (2.0, 0.1))
+    cam = scenes.look_at((0.0, 0.0, -4.0), (0.0, 0.0, 0.0), 130, 70, 100.0)
+    rgb, ft, last = D.forward(g, cam)
+    orgb, oft, olast = O.render_color(g, cam)
+    assert np.array_equal(rgb.view(np.uint32), orgb.view(np.uint32))
+    assert np.array_equal(last, olast)
+
+
+def test_nonfinite_parameter_is_an_error():
+    g = scenes.random_gaussians(100, 29, 1.0, (-4.0, 0.5), (0.0, 1.0))
+    g[7, 1] = np.nan
+    cam = scenes.look_at((0.0, 0.0, -4.0), (0.0, 0.0, 0.0), 32, 32, 40.0)
+    with pytest.raises(R.RgsError) as e:
+        R.render_color(g, cam)
+    assert e.value.code == -4
+
+
+def test_singular_camera_is_an_error():
+    g = scenes.random_gaussians(10, 30, 1.0, (-4.0, 0.5), (0.0, 1.0))
+    cam = R.Camera(32, 32, 30.0, 30.0, 16.0, 16.0, np.zeros((4, 4), np.float32))
+    with pytest.raises(R.RgsError) as e:
+        R.render_color(g, cam)
+    assert e.value.code == -5
+
+
+def test_zero_size_camera_is_an_error():
+    g = scenes.random_gaussians(10, 31, 1.0, (-4.0, 0.5), (0.0, 1.0))
+    cam = R.Camera(0, 32, 30.0, 30.0, 0.0, 16.0, np.eye(4, dtype=np.float32))
+    with pytest.raises(R.RgsError):
+        R.render_color(g, cam)
+
+
+# ---- GpuRenderer drop-in (src/gpu/compute.rs) ----------------------------------------
+def test_gpu_renderer_project_wgsl_math():
+    g = scenes.random_gaussians(3000, 32, 1.0, (-4.0, 0.5), (0.0, 1.5))
+    g[::7, 0:3] *= 8.0  # some behind / far off screen
+    cam = scenes.look_at((0.2, 0.1, -4.0), (0.0, 0.0, 0.0), 200, 150, 220.0)
+    sp, keys = R.GpuRenderer().project(g, cam)
+    osp, okeys = O.project_wgsl(g, cam)
+    assert np.array_equal(keys, okeys)
+    assert np.array_equal(sp.view(np.uint32), osp.view(np.uint32))
+
+
+def test_gpu_renderer_project_cpu_math_matches_cpu_projection():
+    g = scenes.random_gaussians(2000, 33, 1.0, (-4.0, 0.5), (0.0, 1.0))
+    cam = scenes.look_at((0.0, 0.3, -4.0), (0.0, 0.0, 0.0), 160, 120, 180.0)
+    sp, keys = R.GpuRenderer(cpu_math=True).project(g, cam)
+    vis, rec, _ = O.project(g, cam)
+    m = vis.astype(bool)
+    assert np.array_equal(keys[~m], np.full((~m).sum(), 0xFFFFFFFF, np.uint32))
+    ref = np.stack([rec[:, 0], rec[:, 1], rec[:, 2], rec[:, 3], rec[:, 4], rec[:, 8], rec[:, 9], rec[:, 10], rec[:, 14], rec[:, 15]], 1)
+    assert np.array_equal(sp[m].view(np.uint32), ref[m].view(np.uint32))
+
+
+def test_gpu_smoke_ported():
+    """tests/gpu_smoke.rs:113-143 on the CUDA projection."""
+    from tests import refcases as RC
+
+    cam = O.identity_camera(32, 32)
+    g = RC.gaussian_new([0.0, 0.0, 2.0])
+    g[3] = RC.logit(0.9)
+    g[8:11] = -1.5
+    g[11] = 1.0
+    sp, _ = R.GpuRenderer().project(g[None], cam)
+    assert sp.shape == (1, 10)
+    assert sp[0, 8] > 0.0 and sp[0, 9] > 0.0
+    assert np.isfinite(sp[0, 0]) and np.isfinite(sp[0, 1])
+
+
+def test_gpu_renderer_render_matches_cpu_composite():
+    """GpuRenderer::render (src/gpu/compute.rs:210-218): WGSL projection + the
+    CPU compositor of compute.rs:243-296, here composited on the GPU."""
+    g = scenes.random_gaussians(3000, 34, 1.0, (-3.5, 0.5), (0.0, 1.0))
+    cam = scenes.look_at((0.1, 0.0, -4.0), (0.0, 0.0, 0.0), 190, 130, 200.0)
+    for cpu_math in (False, True):
+        r = R.GpuRenderer(cpu_math=cpu_math)
+        img = r.render(g, cam, (0.1, 0.2, 0.3))
+        sp, _ = r.project(g, cam)
+        ref = O.composite(sp, cam.width, cam.height, (0.1, 0.2, 0.3))
+        assert np.abs(img - ref).max() <= IMG_TOL
+        assert np.array_equal(img.view(np.uint32), ref.view(np.uint32))
+
+
+def test_gpu_smoke_render_lit_center():
+    """tests/gpu_smoke.rs:136-139: the full GPU render lights the centre pixel."""
+    from tests import refcases as RC
+
+    cam = O.identity_camera(32, 32)
+    g = RC.gaussian_new([0.0, 0.0, 2.0])
+    g[3] = RC.logit(0.9)
+    g[8:11] = -1.5
+    g[11] = 1.0
+    img = R.GpuRenderer().render(g[None], cam)
+    assert img[16, 16, 0] > 0.0
+
+
+def test_stage_profiling_and_external_stream():
+    import torch
+
+    g, cams, targets = multi_view_scene(n=1500, seed=35)
+    tr = R.Trainer(g, cams, targets)
+    s = torch.cuda.Stream()
+    tr.ctx.set_stream(s.cuda_stream)
+    tr.ctx.set_profiling(True)
+    tr.step([0, 1, 2], mode=R.Trainer.BATCHED)
+    tr.step([3, 4, 5], mode=R.Trainer.PLAIN)
+    ms = tr.ctx.stage_times(reset=True)
+    assert ms["forward"] > 0 and ms["backward"] > 0 and ms["geometry_adam"] > 0
+    tr.ctx.set_stream(None)
+    tr.step([1, 2], mode=R.Trainer.BATCHED)
