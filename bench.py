@@ -382,7 +382,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     peak_src = "measured"
     if not hbm:
         hbm, peak_src = 6650.0, "fallback"
-    per_step_ms = {k: v / args.steps for k, v in stage_ms.items()}
+    per_step_ms = {k: v / args.steps for k, v in stage_ms.items() if v > 0}
     dom = max(per_step_ms, key=per_step_ms.get) if per_step_ms else None
     roofline = None
     stages = {}

@@ -115,7 +115,12 @@ int cuda_fail(rgs_ctx* c, cudaError_t e, const char* what) {
 // Stage boundary i (0 = start, RGS_NUM_STAGES = end) of the step being issued.
 void mark(rgs_ctx* ctx, int i) {
     if (!ctx->prof) return;
-    cudaEventRecord(ctx->ev[i], ctx->st);
+    // inside a stream capture only an "external" record becomes an event-record
+    // node of the graph (a plain record is just a capture dependency)
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(ctx->st, &cs);
+    if (cs == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(ctx->ev[i], ctx->st, cudaEventRecordExternal);
+    else cudaEventRecord(ctx->ev[i], ctx->st);
     ctx->ev_marked[i] = true;
 }
 

@@ -159,7 +159,14 @@ def test_render_and_backward_matches_oracle(ctx, lam, bg):
     g, cam, target = small_scene(seed=9)
     loss, grads = R.render_and_backward(g, cam, target, bg, R.LossConfig(lam), ctx=ctx)
     ref = O.render_and_backward(g, cam, target, bg, lam)
-    assert abs(loss - ref.loss) <= 1e-4 * abs(ref.loss)
+    # The reference accumulates the 3*w*h L1 terms serially in f32
+    # (backward.rs:667-676), which is itself off by ~1e-4 relative here; the
+    # kernels reduce in a tree and per view in f64. Bar: 1e-3 against the f32
+    # restatement, 1e-5 against the same loss evaluated in f64 on the
+    # (bit-identical) rendered image.
+    assert abs(loss - ref.loss) <= 1e-3 * abs(ref.loss)
+    exact, _ = O.photometric_loss_grad(ref.rendered, target, cam.width, cam.height, lam, double=True)
+    assert abs(loss - exact) <= 1e-5 * abs(exact)
     assert_grads_close(grads, ref.grads)
 
 

@@ -37,6 +37,21 @@ def oracle_step(g, cams, targets, views, state, cfg, lam=0.2, bg=(0.0, 0.0, 0.0)
     return np.array(losses, np.float32), total
 
 
+def step_tolerance(rel=2e-3):
+    """Per record float: rel * learning rate (optimizer.rs:175-184 with the
+    reference's flat-index "SH DC" = sh[0..3]). Adam's first steps move each
+    parameter by about lr * sign(g), so gradient differences at the 1e-3 level
+    (atomic summation order) show up as at most rel * lr."""
+    c = R.TrainConfig()
+    lr = np.full(59, c.lr_sh_rest, np.float32)
+    lr[0:3] = c.lr_position
+    lr[3] = c.lr_opacity
+    lr[4:8] = c.lr_rotation
+    lr[8:11] = c.lr_scale
+    lr[11:14] = c.lr_sh_dc
+    return rel * lr
+
+
 def test_trainer_plain_step_matches_oracle():
     g, cams, targets = multi_view_scene()
     tr = R.Trainer(g, cams, targets)
@@ -45,9 +60,9 @@ def test_trainer_plain_step_matches_oracle():
     go = g.copy()
     so = O.AdamState(g.shape[0])
     olosses, _ = oracle_step(go, cams, targets, views, so, O.TrainConfig())
-    assert np.allclose(losses, olosses, rtol=1e-4)
+    assert np.allclose(losses, olosses, rtol=1e-3)
     gt = tr.gaussians()
-    assert np.abs(gt - go).max() < 1e-6
+    assert (np.abs(gt - go) <= step_tolerance()[None, :]).all()
     st = tr.adam_state()
     assert st.t == 1
     assert np.array_equal(st.grad_denom[: g.shape[0]], so.grad_denom)
@@ -75,7 +90,7 @@ def test_batched_step_matches_plain_over_several_steps():
         lb = tb.step(vs, mode=R.Trainer.BATCHED)
         assert np.allclose(lp, lb, rtol=1e-4, atol=1e-7)
     a, b = tp.gaussians(), tb.gaussians()
-    assert np.abs(a - b).max() < 1e-5
+    assert (np.abs(a - b) <= len(steps) * step_tolerance()[None, :]).all()
     sa, sb = tp.adam_state(), tb.adam_state()
     assert sa.t == sb.t == len(steps)
     assert np.array_equal(sa.grad_denom, sb.grad_denom)
@@ -84,14 +99,14 @@ def test_batched_step_matches_plain_over_several_steps():
 
 def test_batched_pair_overflow_recovers():
     # large footprints: far more (Gaussian, tile) pairs than the initial capacity
-    g, cams, targets = multi_view_scene(n=400, seed=24, log_scale=(-1.0, 0.3))
+    g, cams, targets = multi_view_scene(n=3000, seed=24, log_scale=(-1.2, 0.3))
     tp = R.Trainer(g, cams, targets)
     tb = R.Trainer(g, cams, targets)
     lp = tp.step([0, 1], mode=R.Trainer.PLAIN)
     lb = tb.step([0, 1], mode=R.Trainer.BATCHED)
     assert np.allclose(lp, lb, rtol=1e-4)
     assert tb.ctx.stats()["overflow_retries"] >= 1
-    assert np.abs(tp.gaussians() - tb.gaussians()).max() < 1e-5
+    assert (np.abs(tp.gaussians() - tb.gaussians()) <= step_tolerance()[None, :]).all()
     assert tb.adam_state().t == 1
 
 
