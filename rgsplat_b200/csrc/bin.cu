@@ -11,13 +11,26 @@
 //               search over the sub-tile's offsets in shared memory;
 // then a stable radix sort on the tile id (sort.cu) groups the pairs by tile
 // while keeping depth order inside each tile, and `tile_ranges` records each
-// tile's [start, end).
+// tile's [start, end). Each slot's CTA-tile rectangle comes from the
+// projection as one 8-byte descriptor (first tile id, width | height << 16),
+// the only per-splat gather of these kernels.
 #include "rgs_internal.cuh"
 
 namespace rgs {
 
 constexpr int BIN_THREADS = 256;
 constexpr int BIN_SUB = 1024;  // ranks per emit sub-tile
+
+int bin_grid_blocks() {
+    static int g = 0;
+    if (!g) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        g = sms * 6;
+    }
+    return g;
+}
 
 __device__ __forceinline__ void bin_chunk(uint32_t n, int G, int b, uint32_t& begin, uint32_t& end) {
     uint32_t chunk = (uint32_t)(((uint64_t)n + G - 1) / G);
@@ -27,13 +40,15 @@ __device__ __forceinline__ void bin_chunk(uint32_t n, int G, int b, uint32_t& be
     end = (uint32_t)(bg + chunk < (uint64_t)n ? bg + chunk : (uint64_t)n);
 }
 
-__global__ void __launch_bounds__(BIN_THREADS) k_count_reduce(const uint32_t* __restrict__ order, const uint32_t* __restrict__ cnt,
+__device__ __forceinline__ uint32_t tiles_of(uint2 d) { return (d.y & 0xffffu) * (d.y >> 16); }
+
+__global__ void __launch_bounds__(BIN_THREADS) k_count_reduce(const uint32_t* __restrict__ order, const uint2* __restrict__ tdesc,
                                                               uint32_t S, uint32_t* __restrict__ block_sums) {
     __shared__ uint32_t s_w[BIN_THREADS / 32];
     uint32_t begin, end;
     bin_chunk(S, gridDim.x, blockIdx.x, begin, end);
     uint32_t s = 0;
-    for (uint32_t r = begin + threadIdx.x; r < end; r += BIN_THREADS) s += cnt[order[r]];
+    for (uint32_t r = begin + threadIdx.x; r < end; r += BIN_THREADS) s += tiles_of(tdesc[order[r]]);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = s;
@@ -71,21 +86,20 @@ __global__ void __launch_bounds__(1024) k_scan_block_sums(uint32_t* __restrict__
     if (threadIdx.x == 0) *total = s_carry;
 }
 
-void launch_count_scan(const uint32_t* order, const uint32_t* cnt, uint32_t S, uint32_t* block_sums, uint32_t* total,
-                       int grid, cudaStream_t st) {
-    k_count_reduce<<<grid, BIN_THREADS, 0, st>>>(order, cnt, S, block_sums);
+void launch_count_scan(const uint32_t* order, const uint2* tdesc, uint32_t S, uint32_t* block_sums, uint32_t* total, int grid,
+                       cudaStream_t st) {
+    k_count_reduce<<<grid, BIN_THREADS, 0, st>>>(order, tdesc, S, block_sums);
     k_scan_block_sums<<<1, 1024, 0, st>>>(block_sums, grid, total);
 }
 
-__global__ void __launch_bounds__(BIN_THREADS) k_emit(const uint32_t* __restrict__ order, const uint32_t* __restrict__ cnt,
-                                                      uint32_t S, const uint32_t* __restrict__ block_sums,
-                                                      const float4* __restrict__ rec, const DevCam* __restrict__ cams,
-                                                      uint32_t n_per_view, int tile_w, int tile_h,
-                                                      uint32_t* __restrict__ pkeys, uint32_t* __restrict__ pvals,
-                                                      uint32_t cap, int* __restrict__ overflow,
-                                                      const uint32_t* __restrict__ total, uint32_t* __restrict__ eff) {
+__global__ void __launch_bounds__(BIN_THREADS) k_emit(const uint32_t* __restrict__ order, const uint2* __restrict__ tdesc, uint32_t S,
+                                                      const uint32_t* __restrict__ block_sums, uint32_t* __restrict__ pkeys,
+                                                      uint32_t* __restrict__ pvals, uint32_t cap, int* __restrict__ overflow,
+                                                      const uint32_t* __restrict__ total, uint32_t* __restrict__ eff,
+                                                      const DevCam* __restrict__ cams, uint32_t n_per_view) {
     __shared__ uint32_t s_off[BIN_SUB + 1];
     __shared__ uint32_t s_slot[BIN_SUB];
+    __shared__ uint2 s_desc[BIN_SUB];  // (first tile id, rect width | view tiles_x << 16)
     __shared__ uint32_t s_w[BIN_THREADS / 32];
     constexpr int PER = BIN_SUB / BIN_THREADS;
     int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -100,8 +114,11 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit(const uint32_t* __restrict
         for (int k = 0; k < PER; ++k) {
             uint32_t r = r0 + (uint32_t)(tid * PER + k);
             uint32_t slot = r < end ? order[r] : 0u;
-            c[k] = r < end ? cnt[slot] : 0u;
+            uint2 d = r < end ? tdesc[slot] : make_uint2(0u, 0u);
+            c[k] = tiles_of(d);
             s_slot[tid * PER + k] = slot;
+            if (c[k]) d.y = (d.y & 0xffffu) | ((uint32_t)cams[slot / n_per_view].tiles_x << 16);
+            s_desc[tid * PER + k] = d;
             local += c[k];
         }
         uint32_t x = local;
@@ -127,28 +144,24 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit(const uint32_t* __restrict
         if (tid == 0) s_off[BIN_SUB] = sub_total;
         __syncthreads();
         for (uint32_t q = tid; q < sub_total; q += BIN_THREADS) {
-            // largest r with s_off[r] <= q (entries with zero count are skipped)
+            // largest r with s_off[r] <= q (that entry has a non-zero count)
             int lo = 0, hi = BIN_SUB - 1;
             while (lo < hi) {
                 int mid = (lo + hi + 1) >> 1;
                 if (s_off[mid] <= q) lo = mid;
                 else hi = mid - 1;
             }
-            uint32_t slot = s_slot[lo];
-            uint32_t j = q - s_off[lo];
-            uint32_t v = slot / n_per_view;
-            uint32_t S_ = S;
-            uint32_t rx = __float_as_uint(rec[S_ + slot].w), ry = __float_as_uint(rec[2 * (size_t)S_ + slot].w);
-            int x0 = (int)(rx & 0xffffu), x1 = (int)(rx >> 16), y0 = (int)(ry & 0xffffu);
-            int ctx0 = x0 / tile_w, ctx1 = (x1 + tile_w - 1) / tile_w, cty0 = y0 / tile_h;
-            int wt = ctx1 - ctx0;
-            int tx = ctx0 + (int)(j % (uint32_t)wt), ty = cty0 + (int)(j / (uint32_t)wt);
-            const DevCam& cm = cams[v];
-            uint32_t key = (uint32_t)(cm.tile_base + ty * cm.tiles_x + tx);
+            const uint2 d = s_desc[lo];
+            const uint32_t j = q - s_off[lo];
+            const uint32_t wt = d.y & 0xffffu;
+            const uint32_t row = j / wt;
+            // tile ids of one view are row-major: row r of the rectangle starts
+            // r * tiles_x after its first tile
+            const uint32_t key = d.x + row * (d.y >> 16) + (j - row * wt);
             uint32_t out = base + q;
             if (out < cap) {
                 pkeys[out] = key;
-                pvals[out] = slot;
+                pvals[out] = s_slot[lo];
             } else {
                 *overflow = 1;
             }
@@ -158,13 +171,11 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit(const uint32_t* __restrict
     }
 }
 
-void launch_emit_pairs(const uint32_t* order, const uint32_t* cnt, uint32_t S, const uint32_t* block_sums, const float4* rec,
-                       const DevCam* cams, int nviews, uint32_t n_per_view, int tile_w, int tile_h, uint32_t* pair_keys,
-                       uint32_t* pair_vals, uint32_t cap, int* overflow, const uint32_t* total, uint32_t* eff, int grid,
-                       cudaStream_t st) {
-    (void)nviews;
-    k_emit<<<grid, BIN_THREADS, 0, st>>>(order, cnt, S, block_sums, rec, cams, n_per_view, tile_w, tile_h, pair_keys,
-                                         pair_vals, cap, overflow, total, eff);
+void launch_emit_pairs(const uint32_t* order, const uint2* tdesc, uint32_t S, const uint32_t* block_sums, uint32_t* pair_keys,
+                       uint32_t* pair_vals, uint32_t cap, int* overflow, const uint32_t* total, uint32_t* eff,
+                       const DevCam* cams, uint32_t n_per_view, int grid, cudaStream_t st) {
+    k_emit<<<grid, BIN_THREADS, 0, st>>>(order, tdesc, S, block_sums, pair_keys, pair_vals, cap, overflow, total, eff, cams,
+                                         n_per_view);
 }
 
 __global__ void k_tile_ranges(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ total, uint32_t cap,
@@ -178,10 +189,7 @@ __global__ void k_tile_ranges(const uint32_t* __restrict__ keys, const uint32_t*
 }
 
 void launch_tile_ranges(const uint32_t* pair_keys, const uint32_t* total, uint32_t cap, uint2* ranges, cudaStream_t st) {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    k_tile_ranges<<<sms * 8, 256, 0, st>>>(pair_keys, total, cap, ranges);
+    k_tile_ranges<<<bin_grid_blocks() * 2, 256, 0, st>>>(pair_keys, total, cap, ranges);
 }
 
 }  // namespace rgs

@@ -12,11 +12,20 @@
 //
 // B200 mapping: one CTA per CTA tile (TW x TH pixels, one pixel per thread),
 // persistent CTAs pulling tiles of every view of the batch from one atomic
-// counter; BATCH splat records per round are staged in shared memory and read
-// by all threads as broadcasts. Backward pre-reduces each splat's 9 partial
-// gradients across the warp with shuffles (only when a lane contributed),
-// then across warps with shared-memory atomics, and issues one 3 x 16-byte
-// vector reduction (red.global.add.v4.f32) per splat per CTA.
+// counter. Splat records are staged BATCH at a time in shared memory and read
+// by all threads as broadcasts. The kernels are issue-bound, so work that the
+// reference's own tests would discard is removed without changing any result:
+//   * per splat, alpha < 1/255 is guaranteed once power < thr with
+//     thr = ln(1 / (255 opacity)) - 0.01, so such pixels skip exp;
+//   * per (tile, splat), if the conic's quadratic form is bounded below over
+//     the box of the tile's pixel centres so that power < thr everywhere, the
+//     splat is dropped from the staged batch (the batch is compacted, keeping
+//     each splat's index in the full tile list for last_contrib);
+//   * backward warps skip splats past the warp's largest last_contrib.
+// Backward pre-reduces each splat's 9 partial gradients across the warp with
+// shuffles (only when a lane contributed), across warps with shared-memory
+// atomics, and issues one 3 x 16-byte vector reduction (red.global.add.v4.f32)
+// per splat per CTA.
 //
 // CTA tiles other than 16x16 keep the reference's per-pixel semantics: each
 // record carries its reference-tile rectangle in pixels and a pixel only
@@ -29,10 +38,6 @@
 
 namespace rgs {
 
-// Below this power, opacity <= 1 gives opacity * e^power < 1/255 for every
-// finite opacity, so the reference's own alpha test would skip the splat.
-#define RGS_POWER_CUT (-5.55f)
-
 __device__ __forceinline__ int find_view(const DevCam* cams, int nviews, int tile) {
     int v = 0;
     while (v + 1 < nviews && cams[v + 1].tile_base <= tile) ++v;
@@ -44,12 +49,97 @@ __device__ __forceinline__ bool in_rect(float rx, float ry, int px, int py) {
     return px >= (int)(x & 0xffffu) && px < (int)(x >> 16) && py >= (int)(y & 0xffffu) && py < (int)(y >> 16);
 }
 
+// Power below which alpha = min(op * e^power, 0.99) < 1/255 for this opacity
+// (op <= 1 and op >= 1/255 for every projected splat), with a 1 % margin in
+// alpha that covers the rounding of op * exp and of this logarithm.
+__device__ __forceinline__ float power_floor(float op) { return -__logf(255.0f * op) - 0.01f; }
+
+// Conservative tile test: true only if every pixel centre of the box has
+// power = -q/2 < thr, where q = a dx^2 + 2 b dx dy + c dy^2 (the reference's
+// expression, backward.rs:340). The box minimum of the convex q lies on an
+// edge unless the splat centre is inside; each edge is a 1-D quadratic. Only
+// well-conditioned conics (ac - b^2 >= ac / 100, so the float evaluation of q
+// here and per pixel is accurate to ~1e-4 relative) are tested, with a 1e-3
+// margin; anything else (including NaN) is kept.
+__device__ __forceinline__ bool tile_rejects(float sx, float sy, float a, float b, float c, float thr, float x0c, float x1c,
+                                             float y0c, float y1c) {
+    if (!(a > 0.0f && c > 0.0f && (a * c - b * b) >= 0.01f * (a * c))) return false;
+    const float lx = x0c - sx, hx = x1c - sx, ly = y0c - sy, hy = y1c - sy;
+    if (lx <= 0.0f && hx >= 0.0f && ly <= 0.0f && hy >= 0.0f) return false;
+    float best = __int_as_float(0x7f800000);
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        const float dx = e ? hx : lx;
+        const float dy = fminf(fmaxf(-b * dx / c, ly), hy);
+        best = fminf(best, a * dx * dx + 2.0f * b * dx * dy + c * dy * dy);
+        const float ey = e ? hy : ly;
+        const float ex = fminf(fmaxf(-b * ey / a, lx), hx);
+        best = fminf(best, a * ex * ex + 2.0f * b * ex * ey + c * ey * ey);
+    }
+    return best * 0.999f > -2.0f * thr;
+}
+
+// Stages the tile-list entries [first, end) (at most BATCH) into shared memory,
+// dropping splats the tile test rejects; returns the kept count (block-uniform).
+// li0 is the tile-list index of `first`. Must be called by the whole block.
+// When s_rall is given, every staged entry's pixel rectangle (kept or not) is
+// recorded at its batch position.
+template <int NT, int BATCH>
+__device__ __forceinline__ int stage_batch(const BlendArgs& a, size_t S, uint32_t first, uint32_t end, int li0, float x0c,
+                                           float x1c, float y0c, float y1c, float4* s_a, float4* s_c, float4* s_k, int* s_li,
+                                           uint32_t* s_slot, int* s_wsum, uint2* s_rall) {
+    constexpr int NW = NT / 32;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    int kept = 0;
+#pragma unroll
+    for (int c0 = 0; c0 < BATCH; c0 += NT) {
+        const int j = c0 + tid;
+        const uint32_t idx = first + (uint32_t)j;
+        bool keep = false;
+        float4 A, Q, K;
+        uint32_t slot = 0;
+        if (j < BATCH && idx < end) {
+            slot = a.pair_vals[idx];
+            A = a.rec[slot];
+            Q = a.rec[S + slot];
+            K = a.rec[2 * S + slot];
+            A.w = power_floor(A.z);
+            keep = !tile_rejects(A.x, A.y, Q.x, Q.y, Q.z, A.w, x0c, x1c, y0c, y1c);
+            if (s_rall) s_rall[j] = make_uint2(__float_as_uint(Q.w), __float_as_uint(K.w));
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) s_wsum[w] = __popc(m);
+        __syncthreads();
+        int off = kept, total = 0;
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+            const int t = s_wsum[k];
+            off += k < w ? t : 0;
+            total += t;
+        }
+        if (keep) {
+            const int p = off + __popc(m & ((1u << lane) - 1u));
+            s_a[p] = A;
+            s_c[p] = Q;
+            s_k[p] = K;
+            s_li[p] = li0 + j;
+            if (s_slot) s_slot[p] = slot;
+        }
+        kept += total;
+        __syncthreads();
+    }
+    return kept;
+}
+
 template <int TW, int TH, int BATCH, bool RECT>
 __global__ void __launch_bounds__(TW * TH) k_blend_fwd(BlendArgs a) {
     constexpr int NT = TW * TH;
     __shared__ float4 s_a[BATCH];
     __shared__ float4 s_c[BATCH];
     __shared__ float4 s_k[BATCH];
+    __shared__ int s_li[BATCH];
+    __shared__ int s_wsum[NT / 32];
+    __shared__ uint2 s_rall[RECT ? BATCH : 1];
     __shared__ int s_tile;
     const int tid = threadIdx.x;
     const int total_tiles = a.total_tiles ? (int)*a.total_tiles : a.total_tiles_host;
@@ -66,6 +156,9 @@ __global__ void __launch_bounds__(TW * TH) k_blend_fwd(BlendArgs a) {
         const int px = tx * TW + (tid % TW), py = ty * TH + (tid / TW);
         const bool inside = px < c.width && py < c.height;
         const float pxf = (float)px + 0.5f, pyf = (float)py + 0.5f;
+        // box of the tile's pixel centres
+        const float x0c = (float)(tx * TW) + 0.5f, x1c = (float)(min(tx * TW + TW, c.width) - 1) + 0.5f;
+        const float y0c = (float)(ty * TH) + 0.5f, y1c = (float)(min(ty * TH + TH, c.height) - 1) + 0.5f;
         const uint2 rg = a.ranges[tile];
         float T = 1.0f, C0 = 0.0f, C1 = 0.0f, C2 = 0.0f;
         int last = -1;
@@ -74,36 +167,32 @@ __global__ void __launch_bounds__(TW * TH) k_blend_fwd(BlendArgs a) {
         bool seen = !RECT && rg.y > rg.x;
         for (uint32_t b0 = rg.x; b0 < rg.y; b0 += BATCH) {
             if (__syncthreads_count(!done) == 0) break;
-            for (int j = tid; j < BATCH; j += NT) {
-                uint32_t idx = b0 + j;
-                if (idx < rg.y) {
-                    uint32_t slot = a.pair_vals[idx];
-                    s_a[j] = a.rec[slot];
-                    s_c[j] = a.rec[S + slot];
-                    s_k[j] = a.rec[2 * S + slot];
-                }
+            const bool need_seen = RECT && a.empty_tile_black;
+            const int nb = stage_batch<NT, BATCH>(a, S, b0, rg.y, (int)(b0 - rg.x), x0c, x1c, y0c, y1c, s_a, s_c, s_k, s_li,
+                                                  nullptr, s_wsum, need_seen ? s_rall : nullptr);
+            if (need_seen && !seen) {
+                // the pixel's reference tile list is non-empty iff some entry (kept
+                // or rejected) covers the pixel
+                const int staged = (int)min((uint32_t)BATCH, rg.y - b0);
+                for (int j = 0; j < staged && !seen; ++j)
+                    if (in_rect(__uint_as_float(s_rall[j].x), __uint_as_float(s_rall[j].y), px, py)) seen = true;
             }
-            __syncthreads();
-            const int nb = (int)min((uint32_t)BATCH, rg.y - b0);
-            for (int j = 0; j < nb && !done; ++j) {
-                const float4 A = s_a[j];
-                const float4 Q = s_c[j];
-                if (RECT) {
-                    if (!in_rect(Q.w, s_k[j].w, px, py)) continue;
-                    seen = true;
-                }
+            for (int k = 0; k < nb && !done; ++k) {
+                const float4 A = s_a[k];
+                const float4 Q = s_c[k];
+                if (RECT && !in_rect(Q.w, s_k[k].w, px, py)) continue;
                 const float dx = pxf - A.x, dy = pyf - A.y;
                 const float power = -0.5f * (Q.x * dx * dx + 2.0f * Q.y * dx * dy + Q.z * dy * dy);
-                if (power > 0.0f || power < RGS_POWER_CUT) continue;
+                if (power > 0.0f || power < A.w) continue;
                 const float alpha = fminf(A.z * expf_fast(power), 0.99f);
                 if (alpha < 1.0f / 255.0f) continue;
-                const float4 K = s_k[j];
+                const float4 K = s_k[k];
                 const float weight = alpha * T;
                 C0 += K.x * weight;
                 C1 += K.y * weight;
                 C2 += K.z * weight;
                 T *= 1.0f - alpha;
-                last = (int)(b0 - rg.x) + j;
+                last = s_li[k];
                 if (T < 1e-4f) done = true;
             }
             __syncthreads();
@@ -123,6 +212,38 @@ __global__ void __launch_bounds__(TW * TH) k_blend_fwd(BlendArgs a) {
     }
 }
 
+// Warp sum of nine per-lane values, added into dst[0..8] in shared memory.
+// Values 0..7 are reduced with a transpose (reduce-scatter) pattern: at each
+// xor step a lane keeps half of its values and trades the other half, so after
+// three steps lane l holds value l >> 2 summed over the lanes that differ in
+// bits 4..2, and two more steps finish it: 14 shuffles in place of 45, and
+// eight lanes then add distinct addresses in one instruction.
+__device__ __forceinline__ void warp_reduce_scatter9(const float (&g)[9], int lane, float* dst) {
+    const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+    float w[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float send = b4 ? g[i] : g[i + 4];
+        const float keep = b4 ? g[i + 4] : g[i];
+        w[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+    float x[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const float send = b3 ? w[i] : w[i + 2];
+        const float keep = b3 ? w[i + 2] : w[i];
+        x[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+    float y = (b2 ? x[1] : x[0]) + __shfl_xor_sync(0xffffffffu, b2 ? x[0] : x[1], 4);
+    y += __shfl_xor_sync(0xffffffffu, y, 2);
+    y += __shfl_xor_sync(0xffffffffu, y, 1);
+    float z = g[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) z += __shfl_xor_sync(0xffffffffu, z, o);
+    if ((lane & 3) == 0) atomicAdd(dst + (lane >> 2), y);
+    if (lane == 0) atomicAdd(dst + 8, z);
+}
+
 __device__ __forceinline__ void red_add_v4(float4* addr, float x, float y, float z, float w) {
     asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(addr), "f"(x), "f"(y), "f"(z), "f"(w) : "memory");
 }
@@ -134,8 +255,10 @@ __global__ void __launch_bounds__(TW * TH) k_blend_bwd(BlendArgs a) {
     __shared__ float4 s_a[BATCH];
     __shared__ float4 s_c[BATCH];
     __shared__ float4 s_k[BATCH];
+    __shared__ int s_li[BATCH];
     __shared__ uint32_t s_slot[BATCH];
     __shared__ float s_acc[BATCH][NACC];
+    __shared__ int s_wsum[NT / 32];
     __shared__ int s_tile;
     __shared__ int s_maxlc;
     const int tid = threadIdx.x, lane = tid & 31;
@@ -156,6 +279,8 @@ __global__ void __launch_bounds__(TW * TH) k_blend_bwd(BlendArgs a) {
         const int px = tx * TW + (tid % TW), py = ty * TH + (tid / TW);
         const bool inside = px < c.width && py < c.height;
         const float pxf = (float)px + 0.5f, pyf = (float)py + 0.5f;
+        const float x0c = (float)(tx * TW) + 0.5f, x1c = (float)(min(tx * TW + TW, c.width) - 1) + 0.5f;
+        const float y0c = (float)(ty * TH) + 0.5f, y1c = (float)(min(ty * TH + TH, c.height) - 1) + 0.5f;
         const uint2 rg = a.ranges[tile];
         int lc = -1;
         float T = 0.0f, dl0 = 0.0f, dl1 = 0.0f, dl2 = 0.0f;
@@ -168,36 +293,34 @@ __global__ void __launch_bounds__(TW * TH) k_blend_bwd(BlendArgs a) {
             dl2 = a.dl[pix * 3 + 2];
         }
         float be0 = T * a.bg[0], be1 = T * a.bg[1], be2 = T * a.bg[2];
-        if (lc >= 0) atomicMax(&s_maxlc, lc);
+        const int warp_maxlc = __reduce_max_sync(0xffffffffu, lc);
+        if (lane == 0 && warp_maxlc >= 0) atomicMax(&s_maxlc, warp_maxlc);
         __syncthreads();
         const int maxlc = s_maxlc;
         for (int hi = maxlc; hi >= 0; hi -= BATCH) {
             const int lo = max(hi - BATCH + 1, 0);
-            const int nb = hi - lo + 1;
-            for (int j = tid; j < nb; j += NT) {
-                uint32_t slot = a.pair_vals[rg.x + lo + j];
-                s_slot[j] = slot;
-                s_a[j] = a.rec[slot];
-                s_c[j] = a.rec[S + slot];
-                s_k[j] = a.rec[2 * S + slot];
+            const int nb = stage_batch<NT, BATCH>(a, S, rg.x + (uint32_t)lo, rg.x + (uint32_t)hi + 1u, lo, x0c, x1c, y0c, y1c,
+                                                  s_a, s_c, s_k, s_li, s_slot, s_wsum, nullptr);
+            for (int k = tid; k < nb; k += NT) {
 #pragma unroll
-                for (int k = 0; k < NACC; ++k) s_acc[j][k] = 0.0f;
+                for (int q = 0; q < NACC; ++q) s_acc[k][q] = 0.0f;
             }
             __syncthreads();
-            for (int j = nb - 1; j >= 0; --j) {
-                const int li = lo + j;
+            for (int k = nb - 1; k >= 0; --k) {
+                const int li = s_li[k];
+                if (li > warp_maxlc) continue;  // warp-uniform
                 float g[NACC];
 #pragma unroll
-                for (int k = 0; k < NACC; ++k) g[k] = 0.0f;
+                for (int q = 0; q < NACC; ++q) g[q] = 0.0f;
                 bool contrib = false;
                 if (li <= lc) {
-                    const float4 A = s_a[j];
-                    const float4 Q = s_c[j];
-                    const float4 K = s_k[j];
-                    bool ok = !RECT || in_rect(Q.w, K.w, px, py);
+                    const float4 A = s_a[k];
+                    const float4 Q = s_c[k];
+                    const float4 K = s_k[k];
+                    const bool ok = !RECT || in_rect(Q.w, K.w, px, py);
                     const float dx = pxf - A.x, dy = pyf - A.y;
                     const float power = -0.5f * (Q.x * dx * dx + 2.0f * Q.y * dx * dy + Q.z * dy * dy);
-                    if (ok && power <= 0.0f && power >= RGS_POWER_CUT) {
+                    if (ok && power <= 0.0f && power >= A.w) {
                         const float g_exp = expf_fast(power);
                         const float alpha_raw = A.z * g_exp;
                         const float alpha = fminf(alpha_raw, 0.99f);
@@ -227,28 +350,27 @@ __global__ void __launch_bounds__(TW * TH) k_blend_bwd(BlendArgs a) {
                         }
                     }
                 }
-                if (__any_sync(0xffffffffu, contrib)) {
+                const unsigned cm = __ballot_sync(0xffffffffu, contrib);
+                if (cm != 0u) {
+                    if ((cm & (cm - 1u)) == 0u) {
+                        // a single contributing pixel: add its values directly
+                        if (contrib) {
 #pragma unroll
-                    for (int k = 0; k < NACC; ++k) {
-                        float x = g[k];
-#pragma unroll
-                        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-                        g[k] = x;
-                    }
-                    if (lane == 0) {
-#pragma unroll
-                        for (int k = 0; k < NACC; ++k) atomicAdd(&s_acc[j][k], g[k]);
+                            for (int q = 0; q < NACC; ++q) atomicAdd(&s_acc[k][q], g[q]);
+                        }
+                    } else {
+                        warp_reduce_scatter9(g, lane, &s_acc[k][0]);
                     }
                 }
             }
             __syncthreads();
-            for (int j = tid; j < nb; j += NT) {
-                const float* q = s_acc[j];
+            for (int k = tid; k < nb; k += NT) {
+                const float* q = s_acc[k];
                 bool any = false;
 #pragma unroll
-                for (int k = 0; k < NACC; ++k) any |= (q[k] != 0.0f);
+                for (int i = 0; i < NACC; ++i) any |= (q[i] != 0.0f);
                 if (any) {
-                    uint32_t slot = s_slot[j];
+                    const uint32_t slot = s_slot[k];
                     red_add_v4(a.acc + slot, q[0], q[1], q[2], q[3]);
                     red_add_v4(a.acc + S + slot, q[4], q[5], q[6], q[7]);
                     red_add_v4(a.acc + 2 * S + slot, q[8], 0.0f, 0.0f, 0.0f);

@@ -72,7 +72,7 @@ struct rgs_ctx {
     StepHdr* hdr_h = nullptr;  // pinned
     StepOut* out_h = nullptr;  // pinned
     DBuf outd;      // StepOut (device)
-    DBuf rec, cnt, dkey, ids, acc;
+    DBuf rec, cnt, tdesc, dkey, ids, acc;
     DBuf pkeys, pvals;
     uint32_t pair_cap = 0;
     DBuf ranges, rgb, final_t, last, dl, partials;
@@ -335,6 +335,7 @@ int ensure_work(rgs_ctx* ctx, size_t S, size_t px, size_t tiles, size_t lblocks,
     CK(ctx->rec.ensure(std::max<size_t>(S, 1) * 3 * sizeof(float4)));
     CK(ctx->acc.ensure(std::max<size_t>(S, 1) * 3 * sizeof(float4)));
     CK(ctx->cnt.ensure(std::max<size_t>(S, 1) * 4));
+    CK(ctx->tdesc.ensure(std::max<size_t>(S, 1) * 8));
     CK(ctx->dkey.ensure(std::max<size_t>(S, 1) * 4));
     CK(ctx->ids.ensure(std::max<size_t>(S, 1) * 4));
     CK(ctx->ranges.ensure(std::max<size_t>(tiles, 1) * sizeof(uint2)));
@@ -344,7 +345,7 @@ int ensure_work(rgs_ctx* ctx, size_t S, size_t px, size_t tiles, size_t lblocks,
     CK(ctx->dl.ensure(px * 3 * 4));
     CK(ctx->partials.ensure(std::max<size_t>(lblocks, 1) * 2 * 4));
     CK(ctx->scalars.ensure(SC_COUNT * 4));
-    CK(ctx->block_sums.ensure((size_t)ctx->sort_grid * 4 + 64));
+    CK(ctx->block_sums.ensure((size_t)bin_grid_blocks() * 4 + 64));
     CK(ctx->hdr.ensure(sizeof(StepHdr)));
     CK(ctx->outd.ensure(sizeof(StepOut)));
     (void)V;
@@ -377,7 +378,8 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
     uint32_t* sc = ctx->scalars.as<uint32_t>();
     if (project)
         launch_project(s.params.as<float4>(), s.n, s.cap, cams_dev, V, ctx->opt.tile_w, ctx->opt.tile_h,
-                       ctx->rec.as<float4>(), ctx->cnt.as<uint32_t>(), ctx->dkey.as<uint32_t>(), ctx->ids.as<uint32_t>(), st);
+                       ctx->rec.as<float4>(), ctx->cnt.as<uint32_t>(), ctx->tdesc.as<uint2>(), ctx->dkey.as<uint32_t>(),
+                       ctx->ids.as<uint32_t>(), st);
     mark(ctx, 1);
     cudaError_t e;
     int which = radix_sort_pairs(ctx->dkey.as<uint32_t>(), ctx->ids.as<uint32_t>(), (uint32_t)S, nullptr, 32, ctx->sort,
@@ -385,8 +387,8 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
     if (e != cudaSuccess) return cuda_fail(ctx, e, "depth sort");
     mark(ctx, 2);
     const uint32_t* order = which ? ctx->sort.vals2.as<uint32_t>() : ctx->ids.as<uint32_t>();
-    launch_count_scan(order, ctx->cnt.as<uint32_t>(), (uint32_t)S, ctx->block_sums.as<uint32_t>(), sc + SC_PAIRS,
-                      ctx->sort_grid, st);
+    launch_count_scan(order, ctx->tdesc.as<uint2>(), (uint32_t)S, ctx->block_sums.as<uint32_t>(), sc + SC_PAIRS,
+                      bin_grid_blocks(), st);
     if (host_count) {
         uint32_t K = 0;
         CK(cudaMemcpyAsync(&K, sc + SC_PAIRS, 4, cudaMemcpyDeviceToHost, st));
@@ -414,10 +416,9 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
         }
     }
     CK(cudaMemsetAsync(sc + SC_OVERFLOW, 0, 4, st));
-    launch_emit_pairs(order, ctx->cnt.as<uint32_t>(), (uint32_t)S, ctx->block_sums.as<uint32_t>(), ctx->rec.as<float4>(),
-                      cams_dev, V, (uint32_t)s.n, ctx->opt.tile_w, ctx->opt.tile_h, ctx->pkeys.as<uint32_t>(),
+    launch_emit_pairs(order, ctx->tdesc.as<uint2>(), (uint32_t)S, ctx->block_sums.as<uint32_t>(), ctx->pkeys.as<uint32_t>(),
                       ctx->pvals.as<uint32_t>(), ctx->pair_cap, (int*)(sc + SC_OVERFLOW), sc + SC_PAIRS, sc + SC_PAIRS_EFF,
-                      ctx->sort_grid, st);
+                      cams_dev, (uint32_t)s.n, bin_grid_blocks(), st);
     mark(ctx, 3);
     int which2 = radix_sort_pairs(ctx->pkeys.as<uint32_t>(), ctx->pvals.as<uint32_t>(), ctx->pair_cap, sc + SC_PAIRS_EFF,
                                   bits_for(std::max<size_t>(tiles, 2)), ctx->sort, ctx->sort_grid, st, &e);
@@ -609,7 +610,7 @@ void rgs_destroy(rgs_ctx* ctx) {
         s->params.release(); s->grads.release(); s->m1.release(); s->m2.release(); s->accum.release(); s->denom.release();
     }
     for (auto& t : ctx->targets) t.release();
-    DBuf* bufs[] = {&ctx->hdr, &ctx->outd, &ctx->rec, &ctx->cnt, &ctx->dkey, &ctx->ids, &ctx->acc, &ctx->pkeys, &ctx->pvals,
+    DBuf* bufs[] = {&ctx->hdr, &ctx->outd, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->dkey, &ctx->ids, &ctx->acc, &ctx->pkeys, &ctx->pvals,
                     &ctx->ranges, &ctx->rgb, &ctx->final_t, &ctx->last, &ctx->dl, &ctx->partials, &ctx->scalars,
                     &ctx->block_sums, &ctx->sort.hist, &ctx->sort.keys2, &ctx->sort.vals2, &ctx->dens_scratch,
                     &ctx->dens_out, &ctx->m_tmp, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->stage_d,
@@ -875,7 +876,8 @@ int rgs_gpu_render(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_cam
     launch_project_wgsl(s.params.as<float4>(), (int)n, s.cap, cams_dev, mode == RGS_PROJECT_CPU_MATH ? 1 : 0,
                         ctx->stage_b.as<float>(), ctx->stage_c.as<uint32_t>(), ctx->st);
     launch_composite_prepare(ctx->stage_b.as<float>(), (int)n, cams_dev, ctx->opt.tile_w, ctx->opt.tile_h,
-                             ctx->rec.as<float4>(), ctx->cnt.as<uint32_t>(), ctx->dkey.as<uint32_t>(), ctx->ids.as<uint32_t>(),
+                             ctx->rec.as<float4>(), ctx->cnt.as<uint32_t>(), ctx->tdesc.as<uint2>(), ctx->dkey.as<uint32_t>(),
+                             ctx->ids.as<uint32_t>(),
                              ctx->st);
     Binned b;
     if ((rc = bin_batch(ctx, s, cams_dev, 1, tiles, true, b, false))) return rc;
@@ -1106,7 +1108,7 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
         h->bc[1] = 1.0f - powi_f(tc.beta2, (int)s.t);
         // Everything a captured graph bakes in: sizes, every buffer address, and
         // the loss weight, background and optimiser constants.
-        const DBuf* bufs[] = {&s.params, &s.grads, &s.m1, &s.m2, &s.accum, &s.denom, &ctx->rec, &ctx->cnt, &ctx->dkey,
+        const DBuf* bufs[] = {&s.params, &s.grads, &s.m1, &s.m2, &s.accum, &s.denom, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->dkey,
                               &ctx->ids, &ctx->acc, &ctx->pkeys, &ctx->pvals, &ctx->ranges, &ctx->rgb, &ctx->final_t,
                               &ctx->last, &ctx->dl, &ctx->partials, &ctx->scalars, &ctx->block_sums, &ctx->hdr, &ctx->outd,
                               &ctx->sort.hist, &ctx->sort.keys2, &ctx->sort.vals2};

@@ -118,7 +118,8 @@ __device__ __forceinline__ bool project_one(const float4* __restrict__ params, i
 __global__ void __launch_bounds__(256) k_project(const float4* __restrict__ params, int n, int cap,
                                                  const DevCam* __restrict__ cams, int nviews, int tile_w,
                                                  int tile_h, float4* __restrict__ rec, uint32_t* __restrict__ cnt,
-                                                 uint32_t* __restrict__ dkey, uint32_t* __restrict__ ids) {
+                                                 uint2* __restrict__ tdesc, uint32_t* __restrict__ dkey,
+                                                 uint32_t* __restrict__ ids) {
     size_t S = (size_t)n * nviews;
     size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S) return;
@@ -129,6 +130,7 @@ __global__ void __launch_bounds__(256) k_project(const float4* __restrict__ para
     Projected o;
     if (!project_one<true>(params, cap, i, c, o)) {
         cnt[s] = 0;
+        tdesc[s] = make_uint2(0u, 0u);
         dkey[s] = 0xFFFFFFFFu;
         return;
     }
@@ -144,15 +146,17 @@ __global__ void __launch_bounds__(256) k_project(const float4* __restrict__ para
     rec[S + s] = make_float4(o.conic[0], o.conic[1], o.conic[2], __uint_as_float((uint32_t)x0 | ((uint32_t)x1 << 16)));
     rec[2 * S + s] = make_float4(o.color[0], o.color[1], o.color[2], __uint_as_float((uint32_t)y0 | ((uint32_t)y1 << 16)));
     cnt[s] = (uint32_t)((ctx1 - ctx0) * (cty1 - cty0));
+    tdesc[s] = make_uint2((uint32_t)(c.tile_base + cty0 * c.tiles_x + ctx0),
+                          (uint32_t)(ctx1 - ctx0) | ((uint32_t)(cty1 - cty0) << 16));
     dkey[s] = __float_as_uint(o.depth);
 }
 
 void launch_project(const float4* params, int n, int cap, const DevCam* cams, int nviews, int tile_w, int tile_h,
-                    float4* rec, uint32_t* cnt, uint32_t* dkey, uint32_t* ids, cudaStream_t st) {
+                    float4* rec, uint32_t* cnt, uint2* tdesc, uint32_t* dkey, uint32_t* ids, cudaStream_t st) {
     size_t S = (size_t)n * nviews;
     if (S == 0) return;
     unsigned blocks = (unsigned)((S + 255) / 256);
-    k_project<<<blocks, 256, 0, st>>>(params, n, cap, cams, nviews, tile_w, tile_h, rec, cnt, dkey, ids);
+    k_project<<<blocks, 256, 0, st>>>(params, n, cap, cams, nviews, tile_w, tile_h, rec, cnt, tdesc, dkey, ids);
 }
 
 // ---------------------------------------------------------------------------
@@ -242,14 +246,15 @@ void launch_project_wgsl(const float4* params, int n, int cap, const DevCam* cam
 // The blend kernel then tests each pixel against that box (RECT mode).
 __global__ void __launch_bounds__(256) k_composite_prepare(const float* __restrict__ sp, int n, const DevCam* __restrict__ cam,
                                                            int tile_w, int tile_h, float4* __restrict__ rec,
-                                                           uint32_t* __restrict__ cnt, uint32_t* __restrict__ dkey,
-                                                           uint32_t* __restrict__ ids) {
+                                                           uint32_t* __restrict__ cnt, uint2* __restrict__ tdesc,
+                                                           uint32_t* __restrict__ dkey, uint32_t* __restrict__ ids) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     ids[i] = (uint32_t)i;
     const float* s = sp + (size_t)i * 10;
     const int w = cam->width, h = cam->height;
     cnt[i] = 0;
+    tdesc[i] = make_uint2(0u, 0u);
     dkey[i] = 0xFFFFFFFFu;
     if (!(s[8] >= 1.0f / 255.0f && s[9] > 0.0f)) return;
     float a = s[2], b = s[3], c = s[4];
@@ -271,13 +276,15 @@ __global__ void __launch_bounds__(256) k_composite_prepare(const float* __restri
     rec[(size_t)n + i] = make_float4(a, b, c, __uint_as_float((uint32_t)x0 | ((uint32_t)x1 << 16)));
     rec[2 * (size_t)n + i] = make_float4(s[5], s[6], s[7], __uint_as_float((uint32_t)y0 | ((uint32_t)y1 << 16)));
     cnt[i] = (uint32_t)((ctx1 - ctx0) * (cty1 - cty0));
+    tdesc[i] = make_uint2((uint32_t)(cam->tile_base + cty0 * cam->tiles_x + ctx0),
+                          (uint32_t)(ctx1 - ctx0) | ((uint32_t)(cty1 - cty0) << 16));
     dkey[i] = __float_as_uint(s[9]);
 }
 
 void launch_composite_prepare(const float* splats10, int n, const DevCam* cam, int tile_w, int tile_h, float4* rec,
-                              uint32_t* cnt, uint32_t* dkey, uint32_t* ids, cudaStream_t st) {
+                              uint32_t* cnt, uint2* tdesc, uint32_t* dkey, uint32_t* ids, cudaStream_t st) {
     if (n <= 0) return;
-    k_composite_prepare<<<(n + 255) / 256, 256, 0, st>>>(splats10, n, cam, tile_w, tile_h, rec, cnt, dkey, ids);
+    k_composite_prepare<<<(n + 255) / 256, 256, 0, st>>>(splats10, n, cam, tile_w, tile_h, rec, cnt, tdesc, dkey, ids);
 }
 
 }  // namespace rgs

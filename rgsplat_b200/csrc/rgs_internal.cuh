@@ -114,13 +114,16 @@ void launch_aos_to_grad_planes(const float* aos, float4* planes, int n, int cap,
 void launch_check_finite(const float4* planes, int n, int cap, int* flag, cudaStream_t st);
 
 // project.cu
+// tdesc[s] = (global id of the splat's first CTA tile, width | height << 16 of
+// its CTA-tile rectangle); zero for culled slots.
 void launch_project(const float4* params, int n, int cap, const DevCam* cams, int nviews,
-                    int tile_w, int tile_h, float4* rec, uint32_t* cnt, uint32_t* dkey, uint32_t* ids,
-                    cudaStream_t st);
+                    int tile_w, int tile_h, float4* rec, uint32_t* cnt, uint2* tdesc, uint32_t* dkey,
+                    uint32_t* ids, cudaStream_t st);
 void launch_project_wgsl(const float4* params, int n, int cap, const DevCam* cam, int cpu_math,
                          float* splats10, uint32_t* keys, cudaStream_t st);
 void launch_composite_prepare(const float* splats10, int n, const DevCam* cam, int tile_w, int tile_h,
-                              float4* rec, uint32_t* cnt, uint32_t* dkey, uint32_t* ids, cudaStream_t st);
+                              float4* rec, uint32_t* cnt, uint2* tdesc, uint32_t* dkey, uint32_t* ids,
+                              cudaStream_t st);
 
 // sort.cu: stable LSD radix sort of (key, value) u32 pairs on bits [0, bits).
 // n_dev may be null (then n_host is used). Returns which buffer holds the
@@ -130,12 +133,13 @@ int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n_host, const uint
 int sort_grid_blocks();
 
 // bin.cu
-void launch_count_scan(const uint32_t* order, const uint32_t* cnt, uint32_t S, uint32_t* block_sums,
+void launch_count_scan(const uint32_t* order, const uint2* tdesc, uint32_t S, uint32_t* block_sums,
                        uint32_t* total, int grid, cudaStream_t st);
-void launch_emit_pairs(const uint32_t* order, const uint32_t* cnt, uint32_t S, const uint32_t* block_sums,
-                       const float4* rec, const DevCam* cams, int nviews, uint32_t n_per_view,
-                       int tile_w, int tile_h, uint32_t* pair_keys, uint32_t* pair_vals, uint32_t cap,
-                       int* overflow, const uint32_t* total, uint32_t* eff, int grid, cudaStream_t st);
+void launch_emit_pairs(const uint32_t* order, const uint2* tdesc, uint32_t S, const uint32_t* block_sums,
+                       uint32_t* pair_keys, uint32_t* pair_vals, uint32_t cap, int* overflow,
+                       const uint32_t* total, uint32_t* eff, const DevCam* cams, uint32_t n_per_view,
+                       int grid, cudaStream_t st);
+int bin_grid_blocks();
 void launch_tile_ranges(const uint32_t* pair_keys, const uint32_t* total, uint32_t cap, uint2* ranges,
                         cudaStream_t st);
 
