@@ -72,7 +72,7 @@ struct rgs_ctx {
     StepHdr* hdr_h = nullptr;  // pinned
     StepOut* out_h = nullptr;  // pinned
     DBuf outd;      // StepOut (device)
-    DBuf rec, cnt, tdesc, dkey, ids, acc;
+    DBuf rec, cnt, tdesc, dkey, ids, acc, gv;
     DBuf pkeys, pvals;
     uint32_t pair_cap = 0;
     DBuf ranges, rgb, final_t, last, dl, partials;
@@ -334,6 +334,7 @@ int check_finite(rgs_ctx* ctx, Scene& s) {
 int ensure_work(rgs_ctx* ctx, size_t S, size_t px, size_t tiles, size_t lblocks, int V) {
     CK(ctx->rec.ensure(std::max<size_t>(S, 1) * 3 * sizeof(float4)));
     CK(ctx->acc.ensure(std::max<size_t>(S, 1) * 3 * sizeof(float4)));
+    CK(ctx->gv.ensure(std::max<size_t>(S, 1) * 4 * sizeof(float4)));
     CK(ctx->cnt.ensure(std::max<size_t>(S, 1) * 4));
     CK(ctx->tdesc.ensure(std::max<size_t>(S, 1) * 8));
     CK(ctx->dkey.ensure(std::max<size_t>(S, 1) * 4));
@@ -503,7 +504,7 @@ int run_view_plain(rgs_ctx* ctx, Scene& s, const DevCam& dc_in, const float* tar
     launch_blend_backward(ba, ctx->opt.tile_w, ctx->opt.tile_h, ctx->opt.batch, st);
     mark(ctx, 8);
     launch_geometry(s.params.as<float4>(), s.n, s.cap, cams_dev, 1, ctx->cnt.as<uint32_t>(), ctx->acc.as<float4>(),
-                    s.grads.as<float4>(), accumulate ? 1 : 0, st);
+                    ctx->rec.as<float4>(), ctx->gv.as<float4>(), s.grads.as<float4>(), accumulate ? 1 : 0, st);
     mark(ctx, 9);
     CK(cudaGetLastError());
     if (loss_out) {
@@ -610,7 +611,7 @@ void rgs_destroy(rgs_ctx* ctx) {
         s->params.release(); s->grads.release(); s->m1.release(); s->m2.release(); s->accum.release(); s->denom.release();
     }
     for (auto& t : ctx->targets) t.release();
-    DBuf* bufs[] = {&ctx->hdr, &ctx->outd, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->dkey, &ctx->ids, &ctx->acc, &ctx->pkeys, &ctx->pvals,
+    DBuf* bufs[] = {&ctx->hdr, &ctx->outd, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->dkey, &ctx->ids, &ctx->acc, &ctx->gv, &ctx->pkeys, &ctx->pvals,
                     &ctx->ranges, &ctx->rgb, &ctx->final_t, &ctx->last, &ctx->dl, &ctx->partials, &ctx->scalars,
                     &ctx->block_sums, &ctx->sort.hist, &ctx->sort.keys2, &ctx->sort.vals2, &ctx->dens_scratch,
                     &ctx->dens_out, &ctx->m_tmp, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->stage_d,
@@ -1055,10 +1056,11 @@ int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], fl
             a.denom_inc = (uint32_t)V;
             a.skip_flag = (const int*)(sc + SC_OVERFLOW);
             a.bc_dev = hd->bc;
-            launch_geometry_adam(cams_dev, V, s.n, s.cap, ctx->cnt.as<uint32_t>(), ctx->acc.as<float4>(), a, st);
+            launch_geometry_adam(cams_dev, V, s.n, s.cap, ctx->cnt.as<uint32_t>(), ctx->acc.as<float4>(),
+                                 ctx->rec.as<float4>(), ctx->gv.as<float4>(), a, st);
         } else {
             launch_geometry(s.params.as<float4>(), s.n, s.cap, cams_dev, V, ctx->cnt.as<uint32_t>(), ctx->acc.as<float4>(),
-                            s.grads.as<float4>(), 0, st);
+                            ctx->rec.as<float4>(), ctx->gv.as<float4>(), s.grads.as<float4>(), 0, st);
         }
         mark(ctx, 9);
         cudaMemcpyAsync(&ctx->out_h->pairs, sc + SC_PAIRS, 4, cudaMemcpyDeviceToHost, st);
@@ -1108,7 +1110,7 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
         h->bc[1] = 1.0f - powi_f(tc.beta2, (int)s.t);
         // Everything a captured graph bakes in: sizes, every buffer address, and
         // the loss weight, background and optimiser constants.
-        const DBuf* bufs[] = {&s.params, &s.grads, &s.m1, &s.m2, &s.accum, &s.denom, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->dkey,
+        const DBuf* bufs[] = {&s.params, &s.grads, &s.m1, &s.m2, &s.accum, &s.denom, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->gv, &ctx->dkey,
                               &ctx->ids, &ctx->acc, &ctx->pkeys, &ctx->pvals, &ctx->ranges, &ctx->rgb, &ctx->final_t,
                               &ctx->last, &ctx->dl, &ctx->partials, &ctx->scalars, &ctx->block_sums, &ctx->hdr, &ctx->outd,
                               &ctx->sort.hist, &ctx->sort.keys2, &ctx->sort.vals2};

@@ -1,21 +1,29 @@
-// geom.cu -- geometry backward (splat accumulators -> GaussianGrad), Adam, and
-// the fused geometry-backward + Adam kernel of the batched training step.
+// geom.cu -- geometry backward (blend accumulators -> GaussianGrad), Adam, and
+// the fused geometry-backward + Adam of the batched training step.
 //
 // Geometry follows src/cpu/backward.rs:518-638 (`geometry_backprop`) with
 // src/math/covariance.rs:42-84 (`backprop_cov3d`), src/math/quaternion.rs:45-70
-// (`rotation_jacobian`) and src/math/sh.rs:68-89 (`sh_basis_grad`). The
-// projected quantities it needs (camera-space mean, low-passed 2D covariance,
-// raw SH colour and basis) are recomputed from the parameters in the same
-// order as project.cu instead of being stored per splat.
-// Adam follows src/pipeline/optimizer.rs:116-163: dense over all N, bias
-// corrected, per-parameter learning rates, quaternion renormalisation, and the
-// densification statistics grad_accum += screen_grad_norm, grad_denom += 1 per
-// view.
+// (`rotation_jacobian`) and src/math/sh.rs:68-89 (`sh_basis_grad`); Adam
+// follows src/pipeline/optimizer.rs:116-163 (dense over all N, bias corrected,
+// per-parameter learning rates, quaternion renormalisation, densification
+// statistics grad_accum += screen_grad_norm, grad_denom += 1 per view).
 //
-// One thread per Gaussian; every parameter plane is a coalesced float4 stream.
-// The fused kernel reads the parameters and moments once, sums the per-view
-// gradients in registers, and writes parameters and moments once: the
-// gradient never touches HBM.
+// Two kernels, so neither holds the whole 59-float gradient and the geometry
+// temporaries at once (register pressure, not FLOPs, bounds this stage):
+//  (A) one thread per visible (view, Gaussian) slot: camera-space mean, the
+//      projection Jacobian, the 2D-covariance and conic back-prop, the 3D
+//      covariance gradient dSigma = T^T G T, the mean gradient including the
+//      SH view-direction term, the clamp mask of the colour gradient. It writes
+//      64 bytes per slot.
+//  (B) one thread per Gaussian: sums its views in view order, back-props the
+//      summed dSigma once (backprop_cov3d is linear in dSigma), forms
+//      d opacity_logit, streams the SH gradient plane by plane
+//      (sum_v mask_v * basis_v, with the basis recomputed from the view
+//      direction) and either applies Adam plane by plane (fused step: the
+//      gradient never reaches HBM) or writes/accumulates the gradient planes.
+// The projected quantities are recomputed from the parameters in project.cu's
+// order; the clamp mask uses the projected colour (clamp(raw) lies strictly
+// inside (0, 1) exactly when raw does).
 #include "rgs_internal.cuh"
 #include "rgs_math.cuh"
 
@@ -49,23 +57,30 @@ __device__ __forceinline__ void sh_basis_grad(const float d[3], float g[16][3]) 
     g[15][0] = SH_C3_6 * 3.0f * (xx - yy); g[15][1] = SH_C3_6 * -6.0f * x * y; g[15][2] = 0.0f;
 }
 
-// Per-Gaussian gradient accumulators (sum over the views of a batch).
-struct GradAcc {
-    float pos[3], rot[4], ls[3], op, screen;
-    float sh[48];
-};
+__device__ __forceinline__ float lane_of(const float4& v, int l) { return l == 0 ? v.x : l == 1 ? v.y : l == 2 ? v.z : v.w; }
 
-// Adds one view's contribution of Gaussian i (whose slot accumulators are
-// a0 = (dcolor, dopacity), a1 = (dconic, dsx), a2.x = dsy) to g.
-__device__ __forceinline__ void geometry_one(const float4* __restrict__ params, int cap, int i, const DevCam& c,
-                                             float4 a0, float4 a1, float4 a2, GradAcc& g) {
-    float4 p0 = params[i];
-    float4 p1 = params[(size_t)cap + i];
-    float4 p2 = params[2 * (size_t)cap + i];
-    float pos[3] = {p0.x, p0.y, p0.z};
-    float q[4] = {p1.x, p1.y, p1.z, p1.w};
-    float sc[3] = {exp_cr(p2.x), exp_cr(p2.y), exp_cr(p2.z)};
-    float op = sigmoid(p0.w);
+// ---------------------------------------------------------------------------
+// (A) per (view, Gaussian) slot
+//   gv[0][s] = (d position xyz, d opacity (before the sigmoid factor))
+//   gv[1][s] = (dSigma00, dSigma01, dSigma02, dSigma11)
+//   gv[2][s] = (dSigma12, dSigma22, screen_grad_norm, mask * dcolor r)
+//   gv[3][s] = (mask * dcolor g, mask * dcolor b, 0, 0)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_geom_view(const float4* __restrict__ params, int n, int cap, const DevCam* __restrict__ cams,
+                                                   int nviews, const uint32_t* __restrict__ cnt, const float4* __restrict__ acc,
+                                                   const float4* __restrict__ rec, float4* __restrict__ gv) {
+    const size_t S = (size_t)n * nviews;
+    const size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S || cnt[s] == 0) return;
+    const int v = (int)(s / (size_t)n);
+    const int i = (int)(s - (size_t)v * n);
+    const DevCam& c = cams[v];
+    const float4 a0 = acc[s], a1 = acc[S + s], a2 = acc[2 * S + s];
+    const float4 col = rec[2 * S + s];
+    const float4 p0 = params[i], p1 = params[(size_t)cap + i], p2 = params[2 * (size_t)cap + i];
+    const float pos[3] = {p0.x, p0.y, p0.z};
+    const float q[4] = {p1.x, p1.y, p1.z, p1.w};
+    const float sc[3] = {exp_cr(p2.x), exp_cr(p2.y), exp_cr(p2.z)};
     float pc[3];
     cam_mul_g(c, pos, pc);
     const float fx = c.fx, fy = c.fy;
@@ -74,209 +89,124 @@ __device__ __forceinline__ void geometry_one(const float4* __restrict__ params, 
     for (int r = 0; r < 3; ++r)
 #pragma unroll
         for (int k = 0; k < 3; ++k) V.m[r][k] = c.view[r * 4 + k];
-    M3 sigma3d = build_cov3d(sc, q);
-    // 2D covariance exactly as in projection (projection.rs:24-69)
+    const M3 sig = build_cov3d(sc, q);
+    // projection.rs:24-69 (the projection clamps tz; visible splats have tz > 0.001)
+    const float tx = pc[0], ty = pc[1], tz = pc[2];
+    const float tzc = fmaxf(tz, 0.001f);
     float a2d, b2d, c2d;
     {
-        float tzc = fmaxf(pc[2], 0.001f);
-        M3 j = {{{fx / tzc, 0.0f, -fx * pc[0] / (tzc * tzc)}, {0.0f, fy / tzc, -fy * pc[1] / (tzc * tzc)}, {0.0f, 0.0f, 0.0f}}};
+        M3 j = {{{fx / tzc, 0.0f, -fx * tx / (tzc * tzc)}, {0.0f, fy / tzc, -fy * ty / (tzc * tzc)}, {0.0f, 0.0f, 0.0f}}};
         M3 t = mul(j, V);
-        M3 s2 = mul(mul(t, sigma3d), tr(t));
+        M3 s2 = mul(mul(t, sig), tr(t));
         a2d = s2.m[0][0] + 0.3f;
         b2d = s2.m[0][1];
         c2d = s2.m[1][1] + 0.3f;
     }
-    // opacity (backward.rs:529-531)
-    g.op += a0.w * op * (1.0f - op);
-    // SH (backward.rs:533-544): masked by the [0, 1] clamp of the raw colour
-    float d[3], basis[16];
-    view_dir(pos, c.pos, d);
-    sh_basis(d, basis);
-    float masked[3];
-    float acol[3] = {a0.x, a0.y, a0.z};
-#pragma unroll
-    for (int ch = 0; ch < 3; ++ch) {
-        float acc = 0.0f;
-#pragma unroll
-        for (int kq = 0; kq < 4; ++kq) {
-            float4 v = params[(size_t)(3 + ch * 4 + kq) * cap + i];
-            acc += basis[kq * 4 + 0] * v.x;
-            acc += basis[kq * 4 + 1] * v.y;
-            acc += basis[kq * 4 + 2] * v.z;
-            acc += basis[kq * 4 + 3] * v.w;
-        }
-        float raw = 0.5f + acc;
-        masked[ch] = (raw > 0.0f && raw < 1.0f) ? acol[ch] : 0.0f;
-#pragma unroll
-        for (int k = 0; k < 16; ++k) g.sh[ch * 16 + k] += masked[ch] * basis[k];
-    }
     // conic -> 2D covariance (backward.rs:546-554)
-    float ga = a1.x, gb = a1.y, gc = a1.z;
-    float det = a2d * c2d - b2d * b2d;
-    float det2 = det * det;
-    float dl_da = (-ga * c2d * c2d + gb * b2d * c2d - gc * b2d * b2d) / det2;
-    float dl_db = (2.0f * ga * b2d * c2d - gb * (det + 2.0f * b2d * b2d) + 2.0f * gc * a2d * b2d) / det2;
-    float dl_dc = (-ga * b2d * b2d + gb * a2d * b2d - gc * a2d * a2d) / det2;
-    // 2D covariance -> 3D covariance (backward.rs:556-576)
-    float tx = pc[0], ty = pc[1], tz = pc[2];
-    M3 j = {{{fx / tz, 0.0f, -fx * tx / (tz * tz)}, {0.0f, fy / tz, -fy * ty / (tz * tz)}, {0.0f, 0.0f, 0.0f}}};
-    M3 t_mat = mul(j, V);
-    M3 gcov = {{{dl_da, 0.5f * dl_db, 0.0f}, {0.5f * dl_db, dl_dc, 0.0f}, {0.0f, 0.0f, 0.0f}}};
-    M3 dsig = mul(mul(tr(t_mat), gcov), t_mat);
-    {
-        // covariance.rs:42-84
-        M3 r = to_rotation_matrix(q);
-        M3 m = rs_matrix(sc, q);
-        M3 gs;
+    const float ga = a1.x, gb = a1.y, gc = a1.z;
+    const float det = a2d * c2d - b2d * b2d;
+    const float det2 = det * det;
+    const float dl_da = (-ga * c2d * c2d + gb * b2d * c2d - gc * b2d * b2d) / det2;
+    const float dl_db = (2.0f * ga * b2d * c2d - gb * (det + 2.0f * b2d * b2d) + 2.0f * gc * a2d * b2d) / det2;
+    const float dl_dc = (-ga * b2d * b2d + gb * a2d * b2d - gc * a2d * a2d) / det2;
+    // T = J W, rows u0, u1 (row 2 of J is zero) (backward.rs:556-564)
+    const float j00 = fx / tz, j02 = -fx * tx / (tz * tz), j11 = fy / tz, j12 = -fy * ty / (tz * tz);
+    float u0[3], u1[3];
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int b = 0; b < 3; ++b) gs.m[a][b] = dsig.m[a][b] + dsig.m[b][a];
-        M3 dm = mul(gs, m);
-        M3 dr;
-#pragma unroll
-        for (int jj = 0; jj < 3; ++jj) {
-            float acc = 0.0f;
-#pragma unroll
-            for (int ii = 0; ii < 3; ++ii) {
-                acc += dm.m[ii][jj] * r.m[ii][jj];
-                dr.m[ii][jj] = dm.m[ii][jj] * sc[jj];
-            }
-            g.ls[jj] += acc * sc[jj];
-        }
-        float qn[4];
-        qnormalize(q, qn);
-        float w = qn[0], x = qn[1], y = qn[2], z = qn[3];
-        M3 jac[4] = {
-            {{{0.0f, -2.0f * z, 2.0f * y}, {2.0f * z, 0.0f, -2.0f * x}, {-2.0f * y, 2.0f * x, 0.0f}}},
-            {{{0.0f, 2.0f * y, 2.0f * z}, {2.0f * y, -4.0f * x, -2.0f * w}, {2.0f * z, 2.0f * w, -4.0f * x}}},
-            {{{-4.0f * y, 2.0f * x, 2.0f * w}, {2.0f * x, 0.0f, 2.0f * z}, {-2.0f * w, 2.0f * z, -4.0f * y}}},
-            {{{-4.0f * z, -2.0f * w, 2.0f * x}, {2.0f * w, -4.0f * z, 2.0f * y}, {2.0f * x, 2.0f * y, 0.0f}}},
-        };
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            float s = 0.0f;
-#pragma unroll
-            for (int cc = 0; cc < 3; ++cc)
-#pragma unroll
-                for (int rr = 0; rr < 3; ++rr) s += jac[k].m[rr][cc] * dr.m[rr][cc];
-            g.rot[k] += s;
-        }
+    for (int k = 0; k < 3; ++k) {
+        u0[k] = j00 * V.m[0][k] + j02 * V.m[2][k];
+        u1[k] = j11 * V.m[1][k] + j12 * V.m[2][k];
     }
-    // mean (backward.rs:578-608)
-    float asx = a1.w, asy = a2.x;
+    // dSigma3D = T^T G T with G = [[dl_da, dl_db/2], [dl_db/2, dl_dc]] (backward.rs:567-573)
+    const float hb = 0.5f * dl_db;
+    float r0[3], r1[3];  // G T rows
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        r0[k] = dl_da * u0[k] + hb * u1[k];
+        r1[k] = hb * u0[k] + dl_dc * u1[k];
+    }
+    float dS[6];  // 00, 01, 02, 11, 12, 22
+    dS[0] = u0[0] * r0[0] + u1[0] * r1[0];
+    dS[1] = u0[0] * r0[1] + u1[0] * r1[1];
+    dS[2] = u0[0] * r0[2] + u1[0] * r1[2];
+    dS[3] = u0[1] * r0[1] + u1[1] * r1[1];
+    dS[4] = u0[1] * r0[2] + u1[1] * r1[2];
+    dS[5] = u0[2] * r0[2] + u1[2] * r1[2];
+    // mean through (sx, sy) and through J(pcam) (backward.rs:578-605)
+    const float asx = a1.w, asy = a2.x;
     float dp[3] = {asx * fx / tz, asy * fy / tz, asx * (-fx * tx / (tz * tz)) + asy * (-fy * ty / (tz * tz))};
     {
-        M3 dj[3] = {
-            {{{0.0f, 0.0f, -fx / (tz * tz)}, {0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}}},
-            {{{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, -fy / (tz * tz)}, {0.0f, 0.0f, 0.0f}}},
-            {{{-fx / (tz * tz), 0.0f, 2.0f * fx * tx / (tz * tz * tz)}, {0.0f, -fy / (tz * tz), 2.0f * fy * ty / (tz * tz * tz)}, {0.0f, 0.0f, 0.0f}}},
-        };
-        M3 sig_tt = mul(sigma3d, tr(t_mat));
-        M3 ts = mul(t_mat, sigma3d);
+        // Sigma u0, Sigma u1, Sigma w2 with w2 = row 2 of W
+        float su0[3], su1[3], sw2[3];
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            su0[r] = sig.m[r][0] * u0[0] + sig.m[r][1] * u0[1] + sig.m[r][2] * u0[2];
+            su1[r] = sig.m[r][0] * u1[0] + sig.m[r][1] * u1[1] + sig.m[r][2] * u1[2];
+            sw2[r] = sig.m[r][0] * V.m[2][0] + sig.m[r][1] * V.m[2][1] + sig.m[r][2] * V.m[2][2];
+        }
+        const float tz2 = tz * tz, tz3 = tz2 * tz;
+        // d/dtx: dT row 0 = -fx/tz^2 w2
+        const float ax = -fx / tz2;
+        const float w2su0 = V.m[2][0] * su0[0] + V.m[2][1] * su0[1] + V.m[2][2] * su0[2];
+        const float w2su1 = V.m[2][0] * su1[0] + V.m[2][1] * su1[1] + V.m[2][2] * su1[2];
+        dp[0] += dl_da * (2.0f * ax * w2su0) + dl_db * (ax * w2su1);
+        // d/dty: dT row 1 = -fy/tz^2 w2
+        const float ay = -fy / tz2;
+        const float u0sw2 = u0[0] * sw2[0] + u0[1] * sw2[1] + u0[2] * sw2[2];
+        dp[1] += dl_db * (ay * u0sw2) + dl_dc * (2.0f * ay * w2su1);
+        // d/dtz: dT row 0 = -fx/tz^2 W0 + 2 fx tx/tz^3 W2, row 1 = -fy/tz^2 W1 + 2 fy ty/tz^3 W2
+        float g0[3], g1[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            M3 dt = mul(dj[k], V);
-            M3 p1m = mul(dt, sig_tt), p2m = mul(ts, tr(dt));
-            float d00 = p1m.m[0][0] + p2m.m[0][0], d01 = p1m.m[0][1] + p2m.m[0][1], d11 = p1m.m[1][1] + p2m.m[1][1];
-            dp[k] += dl_da * d00 + dl_db * d01 + dl_dc * d11;
+            g0[k] = (-fx / tz2) * V.m[0][k] + (2.0f * fx * tx / tz3) * V.m[2][k];
+            g1[k] = (-fy / tz2) * V.m[1][k] + (2.0f * fy * ty / tz3) * V.m[2][k];
         }
+        const float g0su0 = g0[0] * su0[0] + g0[1] * su0[1] + g0[2] * su0[2];
+        const float g0su1 = g0[0] * su1[0] + g0[1] * su1[1] + g0[2] * su1[2];
+        const float g1su0 = g1[0] * su0[0] + g1[1] * su0[1] + g1[2] * su0[2];
+        const float g1su1 = g1[0] * su1[0] + g1[1] * su1[1] + g1[2] * su1[2];
+        dp[2] += dl_da * (2.0f * g0su0) + dl_db * (g0su1 + g1su0) + dl_dc * (2.0f * g1su1);
     }
     float dpos[3];
 #pragma unroll
-    for (int ii = 0; ii < 3; ++ii) dpos[ii] = (V.m[0][ii] * dp[0] + V.m[1][ii] * dp[1]) + V.m[2][ii] * dp[2];
-    // SH view direction (backward.rs:610-632)
-    float u0 = c.pos[0] - pos[0], u1 = c.pos[1] - pos[1], u2 = c.pos[2] - pos[2];
-    float len = sqrtf(u0 * u0 + u1 * u1 + u2 * u2);
-    if (len > 1e-8f) {
-        float dir[3] = {u0 / len, u1 / len, u2 / len};
+    for (int k = 0; k < 3; ++k) dpos[k] = (V.m[0][k] * dp[0] + V.m[1][k] * dp[1]) + V.m[2][k] * dp[2];
+    // colour mask and the SH view-direction term (backward.rs:535-539, 610-632)
+    const float mr = (col.x > 0.0f && col.x < 1.0f) ? a0.x : 0.0f;
+    const float mg = (col.y > 0.0f && col.y < 1.0f) ? a0.y : 0.0f;
+    const float mb = (col.z > 0.0f && col.z < 1.0f) ? a0.z : 0.0f;
+    const float ux = c.pos[0] - pos[0], uy = c.pos[1] - pos[1], uz = c.pos[2] - pos[2];
+    const float len = sqrtf(ux * ux + uy * uy + uz * uz);
+    if (len > 1e-8f && (mr != 0.0f || mg != 0.0f || mb != 0.0f)) {
+        const float dir[3] = {ux / len, uy / len, uz / len};
         float db[16][3];
         sh_basis_grad(dir, db);
         float dd0 = 0.0f, dd1 = 0.0f, dd2 = 0.0f;
 #pragma unroll
-        for (int k = 0; k < 16; ++k) {
-            int pk = 3 + k / 4, lk = k % 4;
-            float4 cr = params[(size_t)pk * cap + i];
-            float4 cg = params[(size_t)(pk + 4) * cap + i];
-            float4 cb = params[(size_t)(pk + 8) * cap + i];
-            float sr = lk == 0 ? cr.x : lk == 1 ? cr.y : lk == 2 ? cr.z : cr.w;
-            float sg = lk == 0 ? cg.x : lk == 1 ? cg.y : lk == 2 ? cg.z : cg.w;
-            float sb = lk == 0 ? cb.x : lk == 1 ? cb.y : lk == 2 ? cb.z : cb.w;
-            float dbk = masked[0] * sr + masked[1] * sg + masked[2] * sb;
-            dd0 += dbk * db[k][0];
-            dd1 += dbk * db[k][1];
-            dd2 += dbk * db[k][2];
+        for (int kq = 0; kq < 4; ++kq) {
+            const float4 cr = params[(size_t)(3 + kq) * cap + i];
+            const float4 cg = params[(size_t)(7 + kq) * cap + i];
+            const float4 cb = params[(size_t)(11 + kq) * cap + i];
+#pragma unroll
+            for (int l = 0; l < 4; ++l) {
+                const int k = kq * 4 + l;
+                const float dbk = mr * lane_of(cr, l) + mg * lane_of(cg, l) + mb * lane_of(cb, l);
+                dd0 += dbk * db[k][0];
+                dd1 += dbk * db[k][1];
+                dd2 += dbk * db[k][2];
+            }
         }
-        float dot = dir[0] * dd0 + dir[1] * dd1 + dir[2] * dd2;
+        const float dot = dir[0] * dd0 + dir[1] * dd1 + dir[2] * dd2;
         dpos[0] += -((dd0 - dir[0] * dot) / len);
         dpos[1] += -((dd1 - dir[1] * dot) / len);
         dpos[2] += -((dd2 - dir[2] * dot) / len);
     }
-    g.pos[0] += dpos[0];
-    g.pos[1] += dpos[1];
-    g.pos[2] += dpos[2];
-    g.screen += sqrtf(asx * asx + asy * asy);
+    gv[s] = make_float4(dpos[0], dpos[1], dpos[2], a0.w);
+    gv[S + s] = make_float4(dS[0], dS[1], dS[2], dS[3]);
+    gv[2 * S + s] = make_float4(dS[4], dS[5], sqrtf(asx * asx + asy * asy), mr);
+    gv[3 * S + s] = make_float4(mg, mb, 0.0f, 0.0f);
 }
 
-__device__ __forceinline__ void zero_acc(GradAcc& g) {
-#pragma unroll
-    for (int k = 0; k < 3; ++k) { g.pos[k] = 0.0f; g.ls[k] = 0.0f; }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) g.rot[k] = 0.0f;
-#pragma unroll
-    for (int k = 0; k < 48; ++k) g.sh[k] = 0.0f;
-    g.op = 0.0f;
-    g.screen = 0.0f;
-}
-
-__device__ __forceinline__ void gather_views(const float4* __restrict__ params, int n, int cap, int i, const DevCam* __restrict__ cams,
-                                             int nviews, const uint32_t* __restrict__ cnt, const float4* __restrict__ acc,
-                                             GradAcc& g) {
-    size_t S = (size_t)n * nviews;
-    for (int v = 0; v < nviews; ++v) {
-        size_t s = (size_t)v * n + i;
-        if (cnt[s] == 0) continue;
-        float4 a0 = acc[s], a1 = acc[S + s], a2 = acc[2 * S + s];
-        geometry_one(params, cap, i, cams[v], a0, a1, a2, g);
-    }
-}
-
-// Plane p of the gradient (same layout as the parameters).
-__device__ __forceinline__ float4 grad_plane(const GradAcc& g, int p) {
-    if (p == 0) return make_float4(g.pos[0], g.pos[1], g.pos[2], g.op);
-    if (p == 1) return make_float4(g.rot[0], g.rot[1], g.rot[2], g.rot[3]);
-    if (p == 2) return make_float4(g.ls[0], g.ls[1], g.ls[2], g.screen);
-    int b = (p - 3) * 4;
-    return make_float4(g.sh[b], g.sh[b + 1], g.sh[b + 2], g.sh[b + 3]);
-}
-
-__global__ void __launch_bounds__(128) k_geometry(const float4* __restrict__ params, int n, int cap, const DevCam* __restrict__ cams,
-                                                  int nviews, const uint32_t* __restrict__ cnt, const float4* __restrict__ acc,
-                                                  float4* __restrict__ grads, int accumulate) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    GradAcc g;
-    zero_acc(g);
-    gather_views(params, n, cap, i, cams, nviews, cnt, acc, g);
-#pragma unroll
-    for (int p = 0; p < NPL; ++p) {
-        float4 v = grad_plane(g, p);
-        float4* dst = grads + (size_t)p * cap + i;
-        if (accumulate) {
-            float4 o = *dst;
-            v.x += o.x; v.y += o.y; v.z += o.z; v.w += o.w;
-        }
-        *dst = v;
-    }
-}
-
-void launch_geometry(const float4* params, int n, int cap, const DevCam* cams, int nviews, const uint32_t* cnt, const float4* acc,
-                     float4* grads, int accumulate, cudaStream_t st) {
-    if (n <= 0) return;
-    k_geometry<<<(n + 127) / 128, 128, 0, st>>>(params, n, cap, cams, nviews, cnt, acc, grads, accumulate);
-}
-
-// optimizer.rs:138-162 for one Gaussian, given its 15 gradient planes.
+// optimizer.rs:142-147 for one element.
 __device__ __forceinline__ float adam_lane(float p, float g, float& m1, float& m2, float lr, const AdamArgs& a, float bc1,
                                            float bc2) {
     m1 = a.b1 * m1 + a.one_minus_b1 * g;
@@ -287,55 +217,189 @@ __device__ __forceinline__ float adam_lane(float p, float g, float& m1, float& m
     return p - upd;
 }
 
-template <class GradFn>
-__device__ __forceinline__ void adam_gaussian(int i, int cap, const AdamArgs& a, GradFn gf, float screen) {
-    const float bc1 = a.bc_dev ? a.bc_dev[0] : a.bc1;
-    const float bc2 = a.bc_dev ? a.bc_dev[1] : a.bc2;
-#pragma unroll
-    for (int p = 0; p < NPL; ++p) {
-        size_t o = (size_t)p * cap + i;
-        size_t om = (size_t)p * a.mstride + i;
-        float4 pv = a.params[o], g = gf(p), m1 = a.m1[om], m2 = a.m2[om];
-        const float* lr = a.lr + p * 4;
-        pv.x = adam_lane(pv.x, g.x, m1.x, m2.x, lr[0], a, bc1, bc2);
-        pv.y = adam_lane(pv.y, g.y, m1.y, m2.y, lr[1], a, bc1, bc2);
-        pv.z = adam_lane(pv.z, g.z, m1.z, m2.z, lr[2], a, bc1, bc2);
-        if (p != 2) pv.w = adam_lane(pv.w, g.w, m1.w, m2.w, lr[3], a, bc1, bc2);
-        if (p == 1) {
-            float nrm = sqrtf(pv.x * pv.x + pv.y * pv.y + pv.z * pv.z + pv.w * pv.w);
-            if (nrm > 1e-8f) { pv.x /= nrm; pv.y /= nrm; pv.z /= nrm; pv.w /= nrm; }
-        }
-        a.params[o] = pv;
-        a.m1[om] = m1;
-        a.m2[om] = m2;
+// Adam on plane p of Gaussian i (lanes 0..3; plane 2 has only three).
+__device__ __forceinline__ float4 adam_plane(int p, int i, int cap, float4 pv, float4 g, const AdamArgs& a, float bc1, float bc2) {
+    const size_t om = (size_t)p * a.mstride + i;
+    float4 m1 = a.m1[om], m2 = a.m2[om];
+    const float* lr = a.lr + p * 4;
+    pv.x = adam_lane(pv.x, g.x, m1.x, m2.x, lr[0], a, bc1, bc2);
+    pv.y = adam_lane(pv.y, g.y, m1.y, m2.y, lr[1], a, bc1, bc2);
+    pv.z = adam_lane(pv.z, g.z, m1.z, m2.z, lr[2], a, bc1, bc2);
+    if (p != 2) pv.w = adam_lane(pv.w, g.w, m1.w, m2.w, lr[3], a, bc1, bc2);
+    if (p == 1) {
+        // renormalise the quaternion (optimizer.rs:155-162)
+        float nrm = sqrtf(pv.x * pv.x + pv.y * pv.y + pv.z * pv.z + pv.w * pv.w);
+        if (nrm > 1e-8f) { pv.x /= nrm; pv.y /= nrm; pv.z /= nrm; pv.w /= nrm; }
     }
-    a.grad_accum[i] += screen;
-    a.grad_denom[i] += a.denom_inc;
+    a.m1[om] = m1;
+    a.m2[om] = m2;
+    (void)cap;
+    return pv;
 }
 
-__global__ void __launch_bounds__(128) k_geometry_adam(const DevCam* __restrict__ cams, int nviews, int n, int cap,
-                                                       const uint32_t* __restrict__ cnt, const float4* __restrict__ acc, AdamArgs a) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+// (B) per Gaussian. MODE 0: write the gradient planes (accumulate if asked);
+// MODE 1: apply Adam.
+template <int MODE>
+__global__ void __launch_bounds__(128) k_geom_gauss(const float4* __restrict__ params_in, int n, int cap,
+                                                    const DevCam* __restrict__ cams, int nviews, const uint32_t* __restrict__ cnt,
+                                                    const float4* __restrict__ gv, float4* __restrict__ grads, int accumulate,
+                                                    AdamArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    if (a.skip_flag && *a.skip_flag) return;
-    GradAcc g;
-    zero_acc(g);
-    gather_views(a.params, n, cap, i, cams, nviews, cnt, acc, g);
-    adam_gaussian(i, cap, a, [&](int p) { return grad_plane(g, p); }, g.screen);
+    if (MODE == 1 && a.skip_flag && *a.skip_flag) return;
+    const size_t S = (size_t)n * nviews;
+    float bc1 = 0.0f, bc2 = 0.0f;
+    if (MODE == 1) {
+        bc1 = a.bc_dev ? a.bc_dev[0] : a.bc1;
+        bc2 = a.bc_dev ? a.bc_dev[1] : a.bc2;
+    }
+    const float4* params = MODE == 1 ? a.params : params_in;
+    const float4 p0 = params[i];
+    const float pos[3] = {p0.x, p0.y, p0.z};
+    // ---- SH planes: sum_v mask_v[ch] * basis_v, then Adam / store per plane
+#pragma unroll 1
+    for (int kq = 0; kq < 4; ++kq) {
+        float4 gr = make_float4(0.0f, 0.0f, 0.0f, 0.0f), gg = gr, gb = gr;
+        for (int v = 0; v < nviews; ++v) {
+            const size_t s = (size_t)v * n + i;
+            if (cnt[s] == 0) continue;
+            const float4 m2 = gv[2 * S + s], m3 = gv[3 * S + s];
+            const float mr = m2.w, mg = m3.x, mb = m3.y;
+            if (mr == 0.0f && mg == 0.0f && mb == 0.0f) continue;
+            float d[3], basis[16];
+            view_dir(pos, cams[v].pos, d);
+            sh_basis(d, basis);
+            const float b0 = basis[kq * 4 + 0], b1 = basis[kq * 4 + 1], b2 = basis[kq * 4 + 2], b3 = basis[kq * 4 + 3];
+            gr.x += mr * b0; gr.y += mr * b1; gr.z += mr * b2; gr.w += mr * b3;
+            gg.x += mg * b0; gg.y += mg * b1; gg.z += mg * b2; gg.w += mg * b3;
+            gb.x += mb * b0; gb.y += mb * b1; gb.z += mb * b2; gb.w += mb * b3;
+        }
+        const float4 gch[3] = {gr, gg, gb};
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch) {
+            const int p = 3 + ch * 4 + kq;
+            const size_t o = (size_t)p * cap + i;
+            if (MODE == 1) {
+                a.params[o] = adam_plane(p, i, cap, a.params[o], gch[ch], a, bc1, bc2);
+            } else {
+                float4 g = gch[ch];
+                if (accumulate) {
+                    const float4 old = grads[o];
+                    g.x += old.x; g.y += old.y; g.z += old.z; g.w += old.w;
+                }
+                grads[o] = g;
+            }
+        }
+    }
+    // ---- geometry: sums over views
+    float dpos[3] = {0.0f, 0.0f, 0.0f}, dop = 0.0f, dS[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, screen = 0.0f;
+    for (int v = 0; v < nviews; ++v) {
+        const size_t s = (size_t)v * n + i;
+        if (cnt[s] == 0) continue;
+        const float4 x0 = gv[s], x1 = gv[S + s], x2 = gv[2 * S + s];
+        dpos[0] += x0.x; dpos[1] += x0.y; dpos[2] += x0.z; dop += x0.w;
+        dS[0] += x1.x; dS[1] += x1.y; dS[2] += x1.z; dS[3] += x1.w;
+        dS[4] += x2.x; dS[5] += x2.y; screen += x2.z;
+    }
+    const float4 p1 = params[(size_t)cap + i], p2 = params[2 * (size_t)cap + i];
+    const float q[4] = {p1.x, p1.y, p1.z, p1.w};
+    const float sc[3] = {exp_cr(p2.x), exp_cr(p2.y), exp_cr(p2.z)};
+    const float op = sigmoid(p0.w);
+    float d_ls[3] = {0.0f, 0.0f, 0.0f}, d_rot[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    {
+        // backprop_cov3d (covariance.rs:42-84) with dL/dSigma = sum over views
+        const M3 g = {{{dS[0], dS[1], dS[2]}, {dS[1], dS[3], dS[4]}, {dS[2], dS[4], dS[5]}}};
+        const M3 r = to_rotation_matrix(q);
+        const M3 m = rs_matrix(sc, q);
+        M3 gs;
+#pragma unroll
+        for (int x = 0; x < 3; ++x)
+#pragma unroll
+            for (int y = 0; y < 3; ++y) gs.m[x][y] = g.m[x][y] + g.m[y][x];
+        const M3 dm = mul(gs, m);
+        M3 dr;
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj) {
+            float accs = 0.0f;
+#pragma unroll
+            for (int ii = 0; ii < 3; ++ii) {
+                accs += dm.m[ii][jj] * r.m[ii][jj];
+                dr.m[ii][jj] = dm.m[ii][jj] * sc[jj];
+            }
+            d_ls[jj] = accs * sc[jj];
+        }
+        float qn[4];
+        qnormalize(q, qn);
+        const float w = qn[0], x = qn[1], y = qn[2], z = qn[3];
+        // sum over (row, col) of dR/dq_k * dL/dR (quaternion.rs:45-70), column-major order
+        d_rot[0] = (2.0f * z * dr.m[1][0] - 2.0f * y * dr.m[2][0]) + (-2.0f * z * dr.m[0][1] + 2.0f * x * dr.m[2][1]) +
+                   (2.0f * y * dr.m[0][2] - 2.0f * x * dr.m[1][2]);
+        d_rot[1] = (2.0f * y * dr.m[1][0] + 2.0f * z * dr.m[2][0]) + (2.0f * y * dr.m[0][1] - 4.0f * x * dr.m[1][1] + 2.0f * w * dr.m[2][1]) +
+                   (2.0f * z * dr.m[0][2] - 2.0f * w * dr.m[1][2] - 4.0f * x * dr.m[2][2]);
+        d_rot[2] = (-4.0f * y * dr.m[0][0] + 2.0f * x * dr.m[1][0] - 2.0f * w * dr.m[2][0]) + (2.0f * x * dr.m[0][1] + 2.0f * z * dr.m[2][1]) +
+                   (2.0f * w * dr.m[0][2] + 2.0f * z * dr.m[1][2] - 4.0f * y * dr.m[2][2]);
+        d_rot[3] = (-4.0f * z * dr.m[0][0] + 2.0f * w * dr.m[1][0] + 2.0f * x * dr.m[2][0]) +
+                   (-2.0f * w * dr.m[0][1] - 4.0f * z * dr.m[1][1] + 2.0f * y * dr.m[2][1]) + (2.0f * x * dr.m[0][2] + 2.0f * y * dr.m[1][2]);
+    }
+    const float4 g0 = make_float4(dpos[0], dpos[1], dpos[2], dop * op * (1.0f - op));
+    const float4 g1 = make_float4(d_rot[0], d_rot[1], d_rot[2], d_rot[3]);
+    const float4 g2 = make_float4(d_ls[0], d_ls[1], d_ls[2], screen);
+    if (MODE == 1) {
+        a.params[i] = adam_plane(0, i, cap, p0, g0, a, bc1, bc2);
+        a.params[(size_t)cap + i] = adam_plane(1, i, cap, p1, g1, a, bc1, bc2);
+        a.params[2 * (size_t)cap + i] = adam_plane(2, i, cap, p2, g2, a, bc1, bc2);
+        a.grad_accum[i] += screen;
+        a.grad_denom[i] += a.denom_inc;
+    } else {
+        const float4 gs3[3] = {g0, g1, g2};
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+            float4 g = gs3[p];
+            const size_t o = (size_t)p * cap + i;
+            if (accumulate) {
+                const float4 old = grads[o];
+                g.x += old.x; g.y += old.y; g.z += old.z; g.w += old.w;
+            }
+            grads[o] = g;
+        }
+    }
 }
 
-void launch_geometry_adam(const DevCam* cams, int nviews, int n, int cap, const uint32_t* cnt, const float4* acc, const AdamArgs& a,
-                          cudaStream_t st) {
+static void launch_geom_view(const float4* params, int n, int cap, const DevCam* cams, int nviews, const uint32_t* cnt,
+                             const float4* acc, const float4* rec, float4* gv, cudaStream_t st) {
+    size_t S = (size_t)n * nviews;
+    if (S == 0) return;
+    k_geom_view<<<(unsigned)((S + 127) / 128), 128, 0, st>>>(params, n, cap, cams, nviews, cnt, acc, rec, gv);
+}
+
+void launch_geometry(const float4* params, int n, int cap, const DevCam* cams, int nviews, const uint32_t* cnt, const float4* acc,
+                     const float4* rec, float4* gv, float4* grads, int accumulate, cudaStream_t st) {
     if (n <= 0) return;
-    k_geometry_adam<<<(n + 127) / 128, 128, 0, st>>>(cams, nviews, n, cap, cnt, acc, a);
+    launch_geom_view(params, n, cap, cams, nviews, cnt, acc, rec, gv, st);
+    AdamArgs a{};
+    k_geom_gauss<0><<<(n + 127) / 128, 128, 0, st>>>(params, n, cap, cams, nviews, cnt, gv, grads, accumulate, a);
+}
+
+void launch_geometry_adam(const DevCam* cams, int nviews, int n, int cap, const uint32_t* cnt, const float4* acc, const float4* rec,
+                          float4* gv, const AdamArgs& a, cudaStream_t st) {
+    if (n <= 0) return;
+    launch_geom_view(a.params, n, cap, cams, nviews, cnt, acc, rec, gv, st);
+    k_geom_gauss<1><<<(n + 127) / 128, 128, 0, st>>>(nullptr, n, cap, cams, nviews, cnt, gv, nullptr, 0, a);
 }
 
 __global__ void __launch_bounds__(256) k_adam(int n, int cap, const float4* __restrict__ grads, AdamArgs a) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (a.skip_flag && *a.skip_flag) return;
-    float screen = grads[2 * (size_t)cap + i].w;
-    adam_gaussian(i, cap, a, [&](int p) { return grads[(size_t)p * cap + i]; }, screen);
+    const float bc1 = a.bc_dev ? a.bc_dev[0] : a.bc1;
+    const float bc2 = a.bc_dev ? a.bc_dev[1] : a.bc2;
+#pragma unroll 1
+    for (int p = 0; p < NPL; ++p) {
+        const size_t o = (size_t)p * cap + i;
+        a.params[o] = adam_plane(p, i, cap, a.params[o], grads[o], a, bc1, bc2);
+    }
+    a.grad_accum[i] += grads[2 * (size_t)cap + i].w;
+    a.grad_denom[i] += a.denom_inc;
 }
 
 void launch_adam(int n, int cap, const float4* grads, const AdamArgs& a, cudaStream_t st) {

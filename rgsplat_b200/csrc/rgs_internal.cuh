@@ -185,11 +185,12 @@ struct AdamArgs {
     const float* bc_dev;    // when non-null, (bc1, bc2) are read from device memory
     int mstride;            // plane stride (Gaussians) of m1 / m2
 };
+// gv: per-slot scratch of 4 float4 planes (S = n * nviews slots).
 void launch_geometry(const float4* params, int n, int cap, const DevCam* cams, int nviews,
-                     const uint32_t* cnt, const float4* acc, float4* grads, int accumulate,
-                     cudaStream_t st);
+                     const uint32_t* cnt, const float4* acc, const float4* rec, float4* gv, float4* grads,
+                     int accumulate, cudaStream_t st);
 void launch_geometry_adam(const DevCam* cams, int nviews, int n, int cap, const uint32_t* cnt,
-                          const float4* acc, const AdamArgs& a, cudaStream_t st);
+                          const float4* acc, const float4* rec, float4* gv, const AdamArgs& a, cudaStream_t st);
 void launch_adam(int n, int cap, const float4* grads, const AdamArgs& a, cudaStream_t st);
 void launch_reset_opacities(float4* params, int n, int cap, cudaStream_t st);
 
