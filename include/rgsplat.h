@@ -99,6 +99,7 @@ typedef struct rgs_options {
                              compacted on prune, optimizer.rs:97-105; "SH DC" lr applies to
                              flat indices 11..13, optimizer.rs:181). 0: moments follow their
                              Gaussians and lr_sh_dc applies to sh[0], sh[16], sh[32]. */
+    int pixels_per_thread; /* blend kernels: 1 or 2 (default) vertically adjacent pixels */
 } rgs_options;
 
 /* Step modes of rgs_trainer_step. */

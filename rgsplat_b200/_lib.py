@@ -99,6 +99,7 @@ class rgs_options(C.Structure):
         ("tile_h", C.c_int),
         ("batch", C.c_int),
         ("reference_compat", C.c_int),
+        ("pixels_per_thread", C.c_int),
     ]
 
 

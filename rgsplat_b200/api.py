@@ -141,7 +141,8 @@ class AdamState:
 class Context:
     """One CUDA stream plus the library's device buffers (``rgs_ctx``)."""
 
-    def __init__(self, device: int = 0, tile: tuple[int, int] = (16, 16), batch: int = 256, reference_compat: bool = True):
+    def __init__(self, device: int = 0, tile: tuple[int, int] = (16, 16), batch: int = 256, reference_compat: bool = True,
+                 pixels_per_thread: int = 2):
         self.lib = L.load()
         o = L.rgs_options()
         self.lib.rgs_options_default(C.byref(o))
@@ -149,6 +150,7 @@ class Context:
         o.tile_w, o.tile_h = int(tile[0]), int(tile[1])
         o.batch = int(batch)
         o.reference_compat = 1 if reference_compat else 0
+        o.pixels_per_thread = int(pixels_per_thread)
         h = C.c_void_p()
         rc = self.lib.rgs_create(C.byref(o), C.byref(h))
         if rc != L.RGS_OK:

@@ -131,9 +131,12 @@ __device__ __forceinline__ int stage_batch(const BlendArgs& a, size_t S, uint32_
     return kept;
 }
 
-template <int TW, int TH, int BATCH, bool RECT>
-__global__ void __launch_bounds__(TW * TH) k_blend_fwd(BlendArgs a) {
-    constexpr int NT = TW * TH;
+// Forward. PPT vertically adjacent pixels per thread share dx and the
+// dx-only products of power, which are evaluated once per (splat, thread) in
+// the reference's rounding order.
+template <int TW, int TH, int BATCH, bool RECT, int PPT>
+__global__ void __launch_bounds__(TW * TH / PPT) k_blend_fwd(BlendArgs a) {
+    constexpr int NT = TW * TH / PPT;
     __shared__ float4 s_a[BATCH];
     __shared__ float4 s_c[BATCH];
     __shared__ float4 s_k[BATCH];
@@ -153,64 +156,89 @@ __global__ void __launch_bounds__(TW * TH) k_blend_fwd(BlendArgs a) {
         const DevCam& c = a.cams[v];
         const int lt = tile - c.tile_base;
         const int tx = lt % c.tiles_x, ty = lt / c.tiles_x;
-        const int px = tx * TW + (tid % TW), py = ty * TH + (tid / TW);
-        const bool inside = px < c.width && py < c.height;
-        const float pxf = (float)px + 0.5f, pyf = (float)py + 0.5f;
+        const int px = tx * TW + (tid % TW), py0 = ty * TH + (tid / TW) * PPT;
+        const float pxf = (float)px + 0.5f;
         // box of the tile's pixel centres
         const float x0c = (float)(tx * TW) + 0.5f, x1c = (float)(min(tx * TW + TW, c.width) - 1) + 0.5f;
         const float y0c = (float)(ty * TH) + 0.5f, y1c = (float)(min(ty * TH + TH, c.height) - 1) + 0.5f;
         const uint2 rg = a.ranges[tile];
-        float T = 1.0f, C0 = 0.0f, C1 = 0.0f, C2 = 0.0f;
-        int last = -1;
-        bool done = !inside;
-        // whether the pixel's reference tile list is non-empty
-        bool seen = !RECT && rg.y > rg.x;
+        float T[PPT], C0[PPT], C1[PPT], C2[PPT];
+        int last[PPT];
+        bool done[PPT], seen[PPT];
+        bool all_done = true;
+#pragma unroll
+        for (int p = 0; p < PPT; ++p) {
+            T[p] = 1.0f;
+            C0[p] = C1[p] = C2[p] = 0.0f;
+            last[p] = -1;
+            done[p] = !(px < c.width && py0 + p < c.height);
+            all_done &= done[p];
+            // whether the pixel's reference tile list is non-empty
+            seen[p] = !RECT && rg.y > rg.x;
+        }
         for (uint32_t b0 = rg.x; b0 < rg.y; b0 += BATCH) {
-            if (__syncthreads_count(!done) == 0) break;
+            if (__syncthreads_count(!all_done) == 0) break;
             const bool need_seen = RECT && a.empty_tile_black;
             const int nb = stage_batch<NT, BATCH>(a, S, b0, rg.y, (int)(b0 - rg.x), x0c, x1c, y0c, y1c, s_a, s_c, s_k, s_li,
                                                   nullptr, s_wsum, need_seen ? s_rall : nullptr);
-            if (need_seen && !seen) {
-                // the pixel's reference tile list is non-empty iff some entry (kept
+            if (need_seen) {
+                // a pixel's reference tile list is non-empty iff some entry (kept
                 // or rejected) covers the pixel
                 const int staged = (int)min((uint32_t)BATCH, rg.y - b0);
-                for (int j = 0; j < staged && !seen; ++j)
-                    if (in_rect(__uint_as_float(s_rall[j].x), __uint_as_float(s_rall[j].y), px, py)) seen = true;
+#pragma unroll
+                for (int p = 0; p < PPT; ++p)
+                    for (int j = 0; j < staged && !seen[p]; ++j)
+                        if (in_rect(__uint_as_float(s_rall[j].x), __uint_as_float(s_rall[j].y), px, py0 + p)) seen[p] = true;
             }
-            for (int k = 0; k < nb && !done; ++k) {
+            for (int k = 0; k < nb && !all_done; ++k) {
                 const float4 A = s_a[k];
                 const float4 Q = s_c[k];
-                if (RECT && !in_rect(Q.w, s_k[k].w, px, py)) continue;
-                const float dx = pxf - A.x, dy = pyf - A.y;
-                const float power = -0.5f * (Q.x * dx * dx + 2.0f * Q.y * dx * dy + Q.z * dy * dy);
-                if (power > 0.0f || power < A.w) continue;
-                const float alpha = fminf(A.z * expf_fast(power), 0.99f);
-                if (alpha < 1.0f / 255.0f) continue;
-                const float4 K = s_k[k];
-                const float weight = alpha * T;
-                C0 += K.x * weight;
-                C1 += K.y * weight;
-                C2 += K.z * weight;
-                T *= 1.0f - alpha;
-                last = s_li[k];
-                if (T < 1e-4f) done = true;
+                const float dx = pxf - A.x;
+                const float tdx = Q.x * dx * dx;
+                const float t2b = 2.0f * Q.y * dx;
+#pragma unroll
+                for (int p = 0; p < PPT; ++p) {
+                    if (done[p]) continue;
+                    if (RECT && !in_rect(Q.w, s_k[k].w, px, py0 + p)) continue;
+                    const float dy = ((float)(py0 + p) + 0.5f) - A.y;
+                    const float power = -0.5f * (tdx + t2b * dy + Q.z * dy * dy);
+                    if (power > 0.0f || power < A.w) continue;
+                    const float alpha = fminf(A.z * expf_fast(power), 0.99f);
+                    if (alpha < 1.0f / 255.0f) continue;
+                    const float4 K = s_k[k];
+                    const float weight = alpha * T[p];
+                    C0[p] += K.x * weight;
+                    C1[p] += K.y * weight;
+                    C2[p] += K.z * weight;
+                    T[p] *= 1.0f - alpha;
+                    last[p] = s_li[k];
+                    if (T[p] < 1e-4f) done[p] = true;
+                }
+                all_done = true;
+#pragma unroll
+                for (int p = 0; p < PPT; ++p) all_done &= done[p];
             }
             __syncthreads();
         }
-        if (inside) {
-            size_t pix = (size_t)c.pix_base + (size_t)py * c.width + px;
-            // forward_pass skips tiles whose list is empty, leaving their pixels
-            // at 0 rather than bg (src/cpu/backward.rs:313-315, 124)
-            const bool black = a.empty_tile_black && !seen;
-            a.rgb[pix * 3 + 0] = black ? 0.0f : C0 + T * a.bg[0];
-            a.rgb[pix * 3 + 1] = black ? 0.0f : C1 + T * a.bg[1];
-            a.rgb[pix * 3 + 2] = black ? 0.0f : C2 + T * a.bg[2];
-            a.final_t[pix] = T;
-            a.last[pix] = last;
+#pragma unroll
+        for (int p = 0; p < PPT; ++p) {
+            const int py = py0 + p;
+            if (px < c.width && py < c.height) {
+                size_t pix = (size_t)c.pix_base + (size_t)py * c.width + px;
+                // forward_pass skips tiles whose list is empty, leaving their pixels
+                // at 0 rather than bg (src/cpu/backward.rs:313-315, 124)
+                const bool black = a.empty_tile_black && !seen[p];
+                a.rgb[pix * 3 + 0] = black ? 0.0f : C0[p] + T[p] * a.bg[0];
+                a.rgb[pix * 3 + 1] = black ? 0.0f : C1[p] + T[p] * a.bg[1];
+                a.rgb[pix * 3 + 2] = black ? 0.0f : C2[p] + T[p] * a.bg[2];
+                a.final_t[pix] = T[p];
+                a.last[pix] = last[p];
+            }
         }
         __syncthreads();
     }
 }
+
 
 // Warp sum of nine per-lane values, added into dst[0..8] in shared memory.
 // Values 0..7 are reduced with a transpose (reduce-scatter) pattern: at each
@@ -248,9 +276,14 @@ __device__ __forceinline__ void red_add_v4(float4* addr, float x, float y, float
     asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(addr), "f"(x), "f"(y), "f"(z), "f"(w) : "memory");
 }
 
-template <int TW, int TH, int BATCH, bool RECT>
-__global__ void __launch_bounds__(TW * TH) k_blend_bwd(BlendArgs a) {
-    constexpr int NT = TW * TH;
+
+// Backward. A thread owns PPT vertical pixels; their gradient contributions to
+// a splat are summed in registers before the warp reduction. T is rebuilt as
+// T * 1/(1 - alpha) (one correctly rounded reciprocal serves both uses; the
+// reference divides, backward.rs:452, which differs by an ulp).
+template <int TW, int TH, int BATCH, bool RECT, int PPT>
+__global__ void __launch_bounds__(TW * TH / PPT) k_blend_bwd(BlendArgs a) {
+    constexpr int NT = TW * TH / PPT;
     constexpr int NACC = 9;
     __shared__ float4 s_a[BATCH];
     __shared__ float4 s_c[BATCH];
@@ -276,24 +309,34 @@ __global__ void __launch_bounds__(TW * TH) k_blend_bwd(BlendArgs a) {
         const DevCam& c = a.cams[v];
         const int lt = tile - c.tile_base;
         const int tx = lt % c.tiles_x, ty = lt / c.tiles_x;
-        const int px = tx * TW + (tid % TW), py = ty * TH + (tid / TW);
-        const bool inside = px < c.width && py < c.height;
-        const float pxf = (float)px + 0.5f, pyf = (float)py + 0.5f;
+        const int px = tx * TW + (tid % TW), py0 = ty * TH + (tid / TW) * PPT;
+        const float pxf = (float)px + 0.5f;
         const float x0c = (float)(tx * TW) + 0.5f, x1c = (float)(min(tx * TW + TW, c.width) - 1) + 0.5f;
         const float y0c = (float)(ty * TH) + 0.5f, y1c = (float)(min(ty * TH + TH, c.height) - 1) + 0.5f;
         const uint2 rg = a.ranges[tile];
-        int lc = -1;
-        float T = 0.0f, dl0 = 0.0f, dl1 = 0.0f, dl2 = 0.0f;
-        if (inside) {
-            size_t pix = (size_t)c.pix_base + (size_t)py * c.width + px;
-            lc = a.last[pix];
-            T = a.final_t[pix];
-            dl0 = a.dl[pix * 3 + 0];
-            dl1 = a.dl[pix * 3 + 1];
-            dl2 = a.dl[pix * 3 + 2];
+        int lc[PPT];
+        float T[PPT], dl0[PPT], dl1[PPT], dl2[PPT], be0[PPT], be1[PPT], be2[PPT];
+        int my_maxlc = -1;
+#pragma unroll
+        for (int p = 0; p < PPT; ++p) {
+            const int py = py0 + p;
+            lc[p] = -1;
+            T[p] = 0.0f;
+            dl0[p] = dl1[p] = dl2[p] = 0.0f;
+            if (px < c.width && py < c.height) {
+                size_t pix = (size_t)c.pix_base + (size_t)py * c.width + px;
+                lc[p] = a.last[pix];
+                T[p] = a.final_t[pix];
+                dl0[p] = a.dl[pix * 3 + 0];
+                dl1[p] = a.dl[pix * 3 + 1];
+                dl2[p] = a.dl[pix * 3 + 2];
+            }
+            be0[p] = T[p] * a.bg[0];
+            be1[p] = T[p] * a.bg[1];
+            be2[p] = T[p] * a.bg[2];
+            my_maxlc = max(my_maxlc, lc[p]);
         }
-        float be0 = T * a.bg[0], be1 = T * a.bg[1], be2 = T * a.bg[2];
-        const int warp_maxlc = __reduce_max_sync(0xffffffffu, lc);
+        const int warp_maxlc = __reduce_max_sync(0xffffffffu, my_maxlc);
         if (lane == 0 && warp_maxlc >= 0) atomicMax(&s_maxlc, warp_maxlc);
         __syncthreads();
         const int maxlc = s_maxlc;
@@ -313,47 +356,52 @@ __global__ void __launch_bounds__(TW * TH) k_blend_bwd(BlendArgs a) {
 #pragma unroll
                 for (int q = 0; q < NACC; ++q) g[q] = 0.0f;
                 bool contrib = false;
-                if (li <= lc) {
+                if (li <= my_maxlc) {
                     const float4 A = s_a[k];
                     const float4 Q = s_c[k];
                     const float4 K = s_k[k];
-                    const bool ok = !RECT || in_rect(Q.w, K.w, px, py);
-                    const float dx = pxf - A.x, dy = pyf - A.y;
-                    const float power = -0.5f * (Q.x * dx * dx + 2.0f * Q.y * dx * dy + Q.z * dy * dy);
-                    if (ok && power <= 0.0f && power >= A.w) {
+                    const float dx = pxf - A.x;
+                    const float tdx = Q.x * dx * dx;
+                    const float t2b = 2.0f * Q.y * dx;
+#pragma unroll
+                    for (int p = 0; p < PPT; ++p) {
+                        if (li > lc[p]) continue;
+                        if (RECT && !in_rect(Q.w, K.w, px, py0 + p)) continue;
+                        const float dy = ((float)(py0 + p) + 0.5f) - A.y;
+                        const float power = -0.5f * (tdx + t2b * dy + Q.z * dy * dy);
+                        if (power > 0.0f || power < A.w) continue;
                         const float g_exp = expf_fast(power);
                         const float alpha_raw = A.z * g_exp;
                         const float alpha = fminf(alpha_raw, 0.99f);
-                        if (alpha >= 1.0f / 255.0f) {
-                            T = T / (1.0f - alpha);
-                            const float weight = alpha * T;
-                            g[0] = dl0 * weight;
-                            g[1] = dl1 * weight;
-                            g[2] = dl2 * weight;
-                            const float inv_1ma = 1.0f / (1.0f - alpha);
-                            float dl_dalpha = 0.0f;
-                            dl_dalpha += dl0 * (T * K.x - be0 * inv_1ma);
-                            dl_dalpha += dl1 * (T * K.y - be1 * inv_1ma);
-                            dl_dalpha += dl2 * (T * K.z - be2 * inv_1ma);
-                            const float dl_draw = dl_dalpha * (alpha_raw > 0.99f ? 0.0f : 1.0f);
-                            g[3] = dl_draw * g_exp;
-                            const float dl_dpower = dl_draw * A.z * g_exp;
-                            g[4] = dl_dpower * (-0.5f * dx * dx);
-                            g[5] = dl_dpower * (-dx * dy);
-                            g[6] = dl_dpower * (-0.5f * dy * dy);
-                            g[7] = dl_dpower * (Q.x * dx + Q.y * dy);
-                            g[8] = dl_dpower * (Q.y * dx + Q.z * dy);
-                            be0 += weight * K.x;
-                            be1 += weight * K.y;
-                            be2 += weight * K.z;
-                            contrib = true;
-                        }
+                        if (alpha < 1.0f / 255.0f) continue;
+                        const float inv_1ma = __frcp_rn(1.0f - alpha);
+                        T[p] = T[p] * inv_1ma;
+                        const float weight = alpha * T[p];
+                        g[0] += dl0[p] * weight;
+                        g[1] += dl1[p] * weight;
+                        g[2] += dl2[p] * weight;
+                        float dl_dalpha = 0.0f;
+                        dl_dalpha += dl0[p] * (T[p] * K.x - be0[p] * inv_1ma);
+                        dl_dalpha += dl1[p] * (T[p] * K.y - be1[p] * inv_1ma);
+                        dl_dalpha += dl2[p] * (T[p] * K.z - be2[p] * inv_1ma);
+                        const float dl_draw = dl_dalpha * (alpha_raw > 0.99f ? 0.0f : 1.0f);
+                        g[3] += dl_draw * g_exp;
+                        const float dl_dpower = dl_draw * A.z * g_exp;
+                        g[4] += dl_dpower * (-0.5f * dx * dx);
+                        g[5] += dl_dpower * (-dx * dy);
+                        g[6] += dl_dpower * (-0.5f * dy * dy);
+                        g[7] += dl_dpower * (Q.x * dx + Q.y * dy);
+                        g[8] += dl_dpower * (Q.y * dx + Q.z * dy);
+                        be0[p] += weight * K.x;
+                        be1[p] += weight * K.y;
+                        be2[p] += weight * K.z;
+                        contrib = true;
                     }
                 }
                 const unsigned cm = __ballot_sync(0xffffffffu, contrib);
                 if (cm != 0u) {
                     if ((cm & (cm - 1u)) == 0u) {
-                        // a single contributing pixel: add its values directly
+                        // a single contributing thread: add its values directly
                         if (contrib) {
 #pragma unroll
                             for (int q = 0; q < NACC; ++q) atomicAdd(&s_acc[k][q], g[q]);
@@ -386,28 +434,29 @@ __global__ void __launch_bounds__(TW * TH) k_blend_bwd(BlendArgs a) {
 typedef void (*BlendKernel)(BlendArgs);
 
 template <int TW, int TH, int BATCH, bool RECT>
-static BlendKernel pick(bool fwd) {
-    return fwd ? (BlendKernel)k_blend_fwd<TW, TH, BATCH, RECT> : (BlendKernel)k_blend_bwd<TW, TH, BATCH, RECT>;
+static BlendKernel pick(bool fwd, int ppt) {
+    if (ppt == 1) return fwd ? (BlendKernel)k_blend_fwd<TW, TH, BATCH, RECT, 1> : (BlendKernel)k_blend_bwd<TW, TH, BATCH, RECT, 1>;
+    return fwd ? (BlendKernel)k_blend_fwd<TW, TH, BATCH, RECT, 2> : (BlendKernel)k_blend_bwd<TW, TH, BATCH, RECT, 2>;
 }
 
 template <int TW, int TH, bool RECT>
-static BlendKernel pick_batch(int batch, bool fwd) {
+static BlendKernel pick_batch(int batch, bool fwd, int ppt) {
     switch (batch) {
-        case 128: return pick<TW, TH, 128, RECT>(fwd);
-        case 512: return pick<TW, TH, 512, RECT>(fwd);
-        default: return pick<TW, TH, 256, RECT>(fwd);
+        case 128: return pick<TW, TH, 128, RECT>(fwd, ppt);
+        case 512: return pick<TW, TH, 512, RECT>(fwd, ppt);
+        default: return pick<TW, TH, 256, RECT>(fwd, ppt);
     }
 }
 
-static BlendKernel select_kernel(int tw, int th, int batch, bool rect, bool fwd) {
-    if (tw == 8 && th == 32) return pick_batch<8, 32, true>(batch, fwd);
-    if (tw == 32 && th == 8) return pick_batch<32, 8, true>(batch, fwd);
-    return rect ? pick_batch<16, 16, true>(batch, fwd) : pick_batch<16, 16, false>(batch, fwd);
+static BlendKernel select_kernel(int tw, int th, int batch, bool rect, bool fwd, int ppt) {
+    if (tw == 8 && th == 32) return pick_batch<8, 32, true>(batch, fwd, ppt);
+    if (tw == 32 && th == 8) return pick_batch<32, 8, true>(batch, fwd, ppt);
+    return rect ? pick_batch<16, 16, true>(batch, fwd, ppt) : pick_batch<16, 16, false>(batch, fwd, ppt);
 }
 
 static int grid_for(BlendKernel k, int threads) {
     static std::mutex mu;
-    static std::pair<BlendKernel, int> cache[64];
+    static std::pair<BlendKernel, int> cache[128];
     static int ncache = 0;
     std::lock_guard<std::mutex> g(mu);
     for (int i = 0; i < ncache; ++i)
@@ -417,14 +466,15 @@ static int grid_for(BlendKernel k, int threads) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k, threads, 0);
     int grid = sms * std::max(per, 1);
-    if (ncache < 64) cache[ncache++] = {k, grid};
+    if (ncache < 128) cache[ncache++] = {k, grid};
     return grid;
 }
 
 static void launch(const BlendArgs& a, int tw, int th, int batch, bool fwd, cudaStream_t st) {
     bool rect = a.rect_filter != 0 || !(tw == REF_TILE && th == REF_TILE);
-    BlendKernel k = select_kernel(tw, th, batch, rect, fwd);
-    int threads = tw * th;
+    int ppt = a.pixels_per_thread == 1 ? 1 : 2;
+    BlendKernel k = select_kernel(tw, th, batch, rect, fwd, ppt);
+    int threads = tw * th / ppt;
     cudaMemsetAsync(a.work, 0, sizeof(uint32_t), st);
     int grid = grid_for(k, threads);
     if (!a.total_tiles) grid = std::min(grid, std::max(a.total_tiles_host, 1));

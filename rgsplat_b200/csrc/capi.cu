@@ -454,6 +454,7 @@ BlendArgs blend_args(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, cons
     a.work = ctx->scalars.as<uint32_t>() + (fwd ? SC_WORK_F : SC_WORK_B);
     a.rect_filter = 0;
     a.empty_tile_black = 1;
+    a.pixels_per_thread = ctx->opt.pixels_per_thread;
     return a;
 }
 
@@ -536,6 +537,7 @@ void rgs_options_default(rgs_options* o) {
     o->tile_h = 16;
     o->batch = 256;
     o->reference_compat = 1;
+    o->pixels_per_thread = 2;
 }
 
 void rgs_train_config_default(rgs_train_config* c) {
@@ -574,6 +576,7 @@ int rgs_create(const rgs_options* opts, rgs_ctx** out) {
     if (opts) o = *opts;
     bool shape_ok = (o.tile_w == 16 && o.tile_h == 16) || (o.tile_w == 8 && o.tile_h == 32) || (o.tile_w == 32 && o.tile_h == 8);
     if (!shape_ok || (o.batch != 128 && o.batch != 256 && o.batch != 512)) return RGS_ERR_INVALID_ARG;
+    if (o.pixels_per_thread != 1 && o.pixels_per_thread != 2) return RGS_ERR_INVALID_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();

@@ -162,6 +162,7 @@ struct BlendArgs {
     uint32_t* work;                // dynamic tile counter (zeroed by the launcher)
     int rect_filter;               // per-pixel reference-tile membership test
     int empty_tile_black;          // pixels of empty reference tiles render 0, not bg
+    int pixels_per_thread;         // 1 or 2 vertically adjacent pixels per thread
 };
 void launch_blend_forward(const BlendArgs& a, int tile_w, int tile_h, int batch, cudaStream_t st);
 void launch_blend_backward(const BlendArgs& a, int tile_w, int tile_h, int batch, cudaStream_t st);

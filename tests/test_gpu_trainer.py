@@ -110,12 +110,12 @@ def test_batched_pair_overflow_recovers():
     assert tb.adam_state().t == 1
 
 
-@pytest.mark.parametrize("tile", [(8, 32), (32, 8)])
+@pytest.mark.parametrize("tile,ppt", [((8, 32), 2), ((32, 8), 2), ((16, 16), 1), ((32, 8), 1)])
 @pytest.mark.parametrize("batch", [128, 512])
-def test_tile_shapes_keep_reference_semantics(tile, batch):
+def test_tile_shapes_keep_reference_semantics(tile, ppt, batch):
     g, cam_list, targets = multi_view_scene(n=3000, seed=25, sizes=((150, 110),), ncams=1)
     cam, target = cam_list[0], targets[0]
-    ctx = R.Context(tile=tile, batch=batch)
+    ctx = R.Context(tile=tile, batch=batch, pixels_per_thread=ppt)
     rgb, ft, _ = D.forward(g, cam, (0.2, 0.1, 0.0), ctx)
     orgb, oft, _ = O.render_color(g, cam, (0.2, 0.1, 0.0))
     assert np.array_equal(rgb.view(np.uint32), orgb.view(np.uint32)), f"max diff {np.abs(rgb - orgb).max()}"
