@@ -135,6 +135,23 @@ int rgs_render_color(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_c
 int rgs_photometric_loss_grad(rgs_ctx* ctx, const float* rendered_rgb, const float* target_rgba, uint32_t width,
                               uint32_t height, float lambda, float* loss_out, float* dl_out);
 
+/* No counterpart in the reference. rgs_photometric_loss_grad on caller-owned
+ * DEVICE buffers for callers that cannot allocate device memory: it allocates
+ * nothing (no context, no cudaMalloc) and keeps its scratch (view descriptor
+ * plus two floats per 32x32 loss block) in a static device array of
+ * 256 + RGS_NOALLOC_MAX_LOSS_BLOCKS * 8 bytes (128.25 KiB) per device, so
+ * images are limited to RGS_NOALLOC_MAX_LOSS_BLOCKS loss blocks (4096x4096
+ * pixels); larger ones return RGS_ERR_CAPACITY. rendered_rgb: w*h*3,
+ * target_rgba: w*h*4, dl_out: w*h*3, loss_out: 1 float, all on `device`.
+ * Work is enqueued on `cuda_stream` (NULL = legacy default stream) and the
+ * call returns without synchronising. Calls that overlap on one device share
+ * the scratch and race: serialise them. On failure a message is written to
+ * err (err_len bytes, may be NULL). */
+#define RGS_NOALLOC_MAX_LOSS_BLOCKS 16384
+int rgs_photometric_loss_grad_noalloc(int device, const float* rendered_rgb, const float* target_rgba,
+                                      uint32_t width, uint32_t height, float lambda, float* loss_out,
+                                      float* dl_out, void* cuda_stream, char* err, size_t err_len);
+
 /* pipeline::optimizer::adam_step (src/pipeline/optimizer.rs:116-163): updates
  * `gaussians` (n * 59) and `state` in place. grads: n * 60. */
 int rgs_adam_step(rgs_ctx* ctx, float* gaussians, size_t n, const float* grads, rgs_adam_state* state,

@@ -131,6 +131,8 @@ SIGNATURES = {
     "rgs_render_and_backward": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), FP, FP, C.POINTER(rgs_loss_config), FP, FP]),
     "rgs_render_color": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), FP, FP]),
     "rgs_photometric_loss_grad": (C.c_int, [CTX, FP, FP, C.c_uint32, C.c_uint32, C.c_float, FP, FP]),
+    "rgs_photometric_loss_grad_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_float,
+                                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t]),
     "rgs_adam_step": (C.c_int, [CTX, FP, C.c_size_t, FP, C.POINTER(rgs_adam_state), C.POINTER(rgs_train_config)]),
     "rgs_densify_and_prune": (C.c_int, [CTX, FP, C.c_size_t, FP, U32P, C.POINTER(rgs_train_config), C.c_float, FP, C.c_size_t, C.POINTER(C.c_size_t)]),
     "rgs_reset_opacities": (C.c_int, [CTX, FP, C.c_size_t]),
