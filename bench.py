@@ -64,6 +64,9 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--tile", default="16x16")
     p.add_argument("--batch", type=int, default=256)
+    p.add_argument("--ppt", type=int, default=2, help="pixels per thread of the blend kernels (1 or 2)")
+    p.add_argument("--no-autotune", action="store_true", help="keep --tile/--batch/--ppt instead of autotuning")
+    p.add_argument("--no-variants", action="store_true", help="skip the recompute vs store-all backward measurement")
     return p.parse_args()
 
 
@@ -159,6 +162,25 @@ def algorithmic_bytes(stage: str, n: int, views: int, pairs: int, pixels: int) -
     if stage == "geometry_adam":
         return n * 240.0 * 3 * 2 + views * n * (48.0 + 4.0)            # params, m1, m2 read + written; accumulators
     return 0.0
+
+
+def measure_backward_variants(R, scenes, device: int, reps: int = 5) -> dict:
+    """Differentiation workload (50k Gaussians, one 512x512 view): the
+    recompute-from-final-T backward against the store-all-T variant, blend
+    kernel times (median of reps, CUDA events) and the blend state each keeps."""
+    cfg = scenes.config(2)
+    g = scenes.make_gaussians(cfg)
+    cam = cfg.cameras[0]
+    ctx = R.Context(device=device)
+    rgb = R.render_color(scenes.perturbed(g, cfg.seed + 1), cam, ctx=ctx)
+    target = np.concatenate([rgb, np.ones((cam.height, cam.width, 1), np.float32)], axis=2)
+    out = {"workload": "50k Gaussians, one 512x512 view"}
+    for name, store in (("recompute", False), ("store_all", True)):
+        reps_out = [R.render_and_backward_variant(g, cam, target, store_all=store, ctx=ctx)[2] for _ in range(reps + 1)][1:]
+        out[name] = {"forward_ms": round(float(np.median([r["forward_ms"] for r in reps_out])), 4),
+                     "backward_ms": round(float(np.median([r["backward_ms"] for r in reps_out])), 4),
+                     "blend_state_bytes": int(reps_out[0]["state_bytes"]), "pairs": int(reps_out[0]["pairs"])}
+    return out
 
 
 def measured_peaks():
@@ -257,7 +279,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local_rank))
 
     tw, th = (int(x) for x in args.tile.split("x"))
-    ctx = R.Context(device=local_rank, tile=(tw, th), batch=args.batch)
+    ctx = R.Context(device=local_rank, tile=(tw, th), batch=args.batch, pixels_per_thread=args.ppt)
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
     cfg, g = build_workload(args.scale)
@@ -299,16 +321,20 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             dist.barrier()
 
     def timed(fn, k: int) -> float:
-        """Seconds for k steps: CUDA events on the library's stream, max over ranks."""
+        """Seconds for k steps: CUDA events on the library's stream, max over ranks.
+        The steps sit in an NVTX range named after fn, so a profiler can select
+        exactly the timed launches (ncu --nvtx --nvtx-include "step_batched/")."""
         barrier()
         torch.cuda.synchronize()
         with torch.cuda.stream(stream):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.nvtx.range_push(fn.__name__)
             e0.record(stream)
             for _ in range(k):
                 fn()
             e1.record(stream)
+            torch.cuda.nvtx.range_pop()
         e1.synchronize()
         barrier()
         torch.cuda.synchronize()
@@ -318,6 +344,16 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             t = float(tt.item())
         return t
+
+    # autotuner: every blend layout timed on the first step's views (results
+    # are identical across layouts), fastest kept
+    tune = None
+    if not args.no_autotune:
+        with torch.cuda.stream(stream):
+            pick, table = trainer.autotune(schedule[0], loss_cfg=lcfg, reps=2)
+        tune = {"chosen": pick, "candidates_ms": table, "measured_on": "render + backward of the first step's views, mean of 2"}
+    opts = ctx.options()
+    layout = (f"{opts['tile_w']}x{opts['tile_h']}", opts["batch"], opts["pixels_per_thread"])
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -354,13 +390,20 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         def step_e2e():
             views = schedule[-1 - (step_e2e.k % 8)]
             step_e2e.k += 1
-            b = 0
-            for v in views:
-                t = pinned_target(v)
+            ts = [pinned_target(v) for v in views]
+            h2d[0] = sum(t.numel() * 4 for t in ts) + len(views) * 100
+            if world == 1:
+                # targets copied from pinned host memory inside the step,
+                # overlapped with projection, sort and forward
+                return trainer.step_host_targets(views, [t.data_ptr() for t in ts], loss_cfg=lcfg, train_cfg=tcfg)
+            for v, t in zip(views, ts):
                 trainer.set_target_ptr(v, t.data_ptr())
-                b += t.numel() * 4
-            h2d[0] = b + len(views) * 100
-            return trainer.step(views, mode=R.Trainer.BATCHED, loss_cfg=lcfg, train_cfg=tcfg)
+            losses = trainer.backward(views, loss_cfg=lcfg, mode=R.Trainer.BATCHED)
+            ptr, nbytes, _ = trainer.grad_buffer()
+            grad = torch.as_tensor(_CudaArray(ptr, nbytes), device=f"cuda:{local_rank}")
+            dist.all_reduce(grad)
+            trainer.apply_adam(tcfg, denom_increment=V * world)
+            return losses
 
         step_e2e.k = 0
         for v in set(x for vs in schedule[-8:] for x in vs):
@@ -416,7 +459,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             "ms_per_step": round(ms_per_step, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "n_gaussians": n, "views_per_step": V, "parallelism": f"view-dp{world}",
-                       "mode": "batched (graph-captured, one launch per stage)", "tile": args.tile, "batch": args.batch,
+                       "mode": "batched (graph-captured, one launch per stage)", "tile": layout[0], "batch": layout[1],
+                       "pixels_per_thread": layout[2], "autotune": tune,
                        "l2": "inputs larger than L2 (236 MB params + 480 MB moments + targets)",
                        "plain_iter_per_s": round(plain_value, 4), "batched_over_plain": round(value / plain_value, 3),
                        "pairs_per_step": int(pairs_last), "pixels_per_step": pixels_per_step},
@@ -427,11 +471,14 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             "cpu_baseline": cpu,
             "clocks": clock_info,
         }
+        if not args.no_variants:
+            line["backward_variants"] = measure_backward_variants(R, scenes, local_rank)
         # kernels launched per batched step: project 1, depth sort 4x3, count
         # scan 2, emit 1, tile sort 3 per 8 bits, ranges 1, forward 1, loss 2,
-        # backward 1, geometry+Adam 1 (+ memsets)
-        tile_bits = max(1, int(np.ceil(np.log2(max(2, V * max(-(-c.width // tw) * -(-c.height // th) for c in cfg.cameras))))))
-        per_step = 1 + 12 + 2 + 1 + 3 * ((tile_bits + 7) // 8) + 1 + 1 + 2 + 1 + 1
+        # backward 1, geometry+Adam 2 (+ memsets)
+        ltw, lth = (int(x) for x in layout[0].split("x"))
+        tile_bits = max(1, int(np.ceil(np.log2(max(2, V * max(-(-c.width // ltw) * -(-c.height // lth) for c in cfg.cameras))))))
+        per_step = 1 + 12 + 2 + 1 + 3 * ((tile_bits + 7) // 8) + 1 + 1 + 2 + 1 + 2
         line["gpu_launches"] = per_step * args.steps
         print(json.dumps(line), flush=True)
     if dist is not None:

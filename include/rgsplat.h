@@ -127,6 +127,27 @@ int rgs_render_and_backward(rgs_ctx* ctx, const float* gaussians, size_t n, cons
                             const float* target_rgba, const float bg[3], const rgs_loss_config* cfg,
                             float* loss_out, float* grads_out);
 
+/* render_and_backward with a chosen blend backward, for the differentiation
+ * study (no counterpart in the reference, whose backward is the recompute
+ * one, src/cpu/backward.rs:391-512):
+ *   RGS_BACKWARD_RECOMPUTE: the library's path -- T is rebuilt from each
+ *     pixel's final T and last contributor; blend state = 8 B per pixel;
+ *   RGS_BACKWARD_STORE_ALL: the forward also stores T before every
+ *     contributing splat at (tile-list position, pixel in tile) and the
+ *     backward reads it; blend state += 1 KiB per (tile, splat) pair (16x16
+ *     tiles only).
+ * report (may be NULL) receives the blend kernel times and state bytes. */
+#define RGS_BACKWARD_RECOMPUTE 0
+#define RGS_BACKWARD_STORE_ALL 1
+typedef struct rgs_backward_report {
+    float forward_ms, backward_ms; /* blend forward / backward kernels, CUDA events */
+    uint64_t state_bytes;          /* device bytes of blend state kept for the backward */
+    uint64_t pairs;                /* (tile, splat) pairs of the view */
+} rgs_backward_report;
+int rgs_render_and_backward_variant(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera,
+                                    const float* target_rgba, const float bg[3], const rgs_loss_config* cfg,
+                                    int variant, float* loss_out, float* grads_out, rgs_backward_report* report);
+
 /* cpu::backward::render_color (src/cpu/backward.rs:152-166): rgb_out w*h*3. */
 int rgs_render_color(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, const float bg[3],
                      float* rgb_out);
@@ -198,6 +219,16 @@ int rgs_trainer_step(rgs_ctx* ctx, const uint32_t* views, size_t nviews, const f
                      const rgs_loss_config* loss_cfg, const rgs_train_config* train_cfg, int mode,
                      float* losses_out);
 
+/* rgs_trainer_step (batched) with each view's RGBA target (w*h*4 f32) read
+ * from caller HOST memory for this step instead of the device-resident
+ * targets: the copies run on a second stream while the step projects, sorts
+ * and renders, and only the loss waits for them. Page-locked host memory lets
+ * the copies overlap; pageable memory works but is copied synchronously. The
+ * buffers may be reused as soon as the call returns. */
+int rgs_trainer_step_host_targets(rgs_ctx* ctx, const uint32_t* views, size_t nviews, const float* const* targets_rgba,
+                                  const float bg[3], const rgs_loss_config* loss_cfg, const rgs_train_config* train_cfg,
+                                  float* losses_out);
+
 /* Render + backward only (mode as for rgs_trainer_step): gradients summed over
  * the views stay on the device for rgs_trainer_get_grads /
  * rgs_trainer_grad_buffer / rgs_trainer_apply_adam. */
@@ -244,6 +275,30 @@ typedef struct rgs_stats {
     uint32_t overflow_retries;
 } rgs_stats;
 int rgs_get_stats(rgs_ctx* ctx, rgs_stats* out);
+
+/* ---- tiling and its autotuner ---------------------------------------------
+ * Tile shape, splats staged per batch and pixels per thread change only how
+ * the blend kernels are laid out, never a result (every combination is
+ * bit-identical), so they may change between training steps. */
+int rgs_get_options(rgs_ctx* ctx, rgs_options* out);
+/* Switches the blend layout (same value sets as rgs_create); the next batched
+ * step recaptures its graph. */
+int rgs_set_tiling(rgs_ctx* ctx, int tile_w, int tile_h, int batch, int pixels_per_thread);
+
+/* One autotuner measurement: device milliseconds per render + backward of the
+ * tuned views (mean of `reps` batched steps without the optimiser update). */
+typedef struct rgs_tune_entry {
+    int tile_w, tile_h, batch, pixels_per_thread;
+    float ms;
+} rgs_tune_entry;
+#define RGS_TUNE_CANDIDATES 18 /* {16x16, 8x32, 32x8} x {128, 256, 512} x {1, 2} */
+/* Times every candidate layout on the trainer's current Gaussians and the
+ * given views (render, loss and backward; parameters and Adam state are not
+ * touched), keeps the fastest and returns it in *chosen. results may be NULL
+ * or hold RGS_TUNE_CANDIDATES entries. */
+int rgs_trainer_autotune(rgs_ctx* ctx, const uint32_t* views, size_t nviews, const float bg[3],
+                         const rgs_loss_config* loss_cfg, int reps, rgs_tune_entry* results,
+                         rgs_options* chosen);
 
 #ifdef __cplusplus
 }

@@ -19,6 +19,7 @@ from .api import (  # noqa: F401
     estimate_scene_extent,
     photometric_loss_grad,
     render_and_backward,
+    render_and_backward_variant,
     render_color,
     reset_opacities,
 )

@@ -113,6 +113,30 @@ class rgs_stats(C.Structure):
     ]
 
 
+class rgs_tune_entry(C.Structure):
+    _fields_ = [
+        ("tile_w", C.c_int),
+        ("tile_h", C.c_int),
+        ("batch", C.c_int),
+        ("pixels_per_thread", C.c_int),
+        ("ms", C.c_float),
+    ]
+
+
+RGS_TUNE_CANDIDATES = 18
+RGS_BACKWARD_RECOMPUTE = 0
+RGS_BACKWARD_STORE_ALL = 1
+
+
+class rgs_backward_report(C.Structure):
+    _fields_ = [
+        ("forward_ms", C.c_float),
+        ("backward_ms", C.c_float),
+        ("state_bytes", C.c_uint64),
+        ("pairs", C.c_uint64),
+    ]
+
+
 _lib = None
 
 FP = C.POINTER(C.c_float)
@@ -129,6 +153,8 @@ SIGNATURES = {
     "rgs_device_count": (C.c_int, [C.POINTER(C.c_int)]),
     "rgs_synchronize": (C.c_int, [CTX]),
     "rgs_render_and_backward": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), FP, FP, C.POINTER(rgs_loss_config), FP, FP]),
+    "rgs_render_and_backward_variant": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), FP, FP, C.POINTER(rgs_loss_config),
+                                                  C.c_int, FP, FP, C.POINTER(rgs_backward_report)]),
     "rgs_render_color": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), FP, FP]),
     "rgs_photometric_loss_grad": (C.c_int, [CTX, FP, FP, C.c_uint32, C.c_uint32, C.c_float, FP, FP]),
     "rgs_photometric_loss_grad_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_float,
@@ -144,6 +170,8 @@ SIGNATURES = {
     "rgs_trainer_set_cameras": (C.c_int, [CTX, C.POINTER(rgs_camera), C.c_size_t]),
     "rgs_trainer_set_target": (C.c_int, [CTX, C.c_size_t, FP]),
     "rgs_trainer_step": (C.c_int, [CTX, U32P, C.c_size_t, FP, C.POINTER(rgs_loss_config), C.POINTER(rgs_train_config), C.c_int, FP]),
+    "rgs_trainer_step_host_targets": (C.c_int, [CTX, U32P, C.c_size_t, C.POINTER(C.c_void_p), FP, C.POINTER(rgs_loss_config),
+                                                C.POINTER(rgs_train_config), FP]),
     "rgs_trainer_backward": (C.c_int, [CTX, U32P, C.c_size_t, FP, C.POINTER(rgs_loss_config), C.c_int, FP]),
     "rgs_trainer_get_grads": (C.c_int, [CTX, FP]),
     "rgs_trainer_grad_buffer": (C.c_int, [CTX, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
@@ -154,6 +182,10 @@ SIGNATURES = {
     "rgs_trainer_get_adam_state": (C.c_int, [CTX, C.POINTER(rgs_adam_state)]),
     "rgs_trainer_set_adam_state": (C.c_int, [CTX, C.POINTER(rgs_adam_state)]),
     "rgs_get_stats": (C.c_int, [CTX, C.POINTER(rgs_stats)]),
+    "rgs_get_options": (C.c_int, [CTX, C.POINTER(rgs_options)]),
+    "rgs_set_tiling": (C.c_int, [CTX, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "rgs_trainer_autotune": (C.c_int, [CTX, U32P, C.c_size_t, FP, C.POINTER(rgs_loss_config), C.c_int,
+                                       C.POINTER(rgs_tune_entry), C.POINTER(rgs_options)]),
     "rgs_set_stream": (C.c_int, [CTX, C.c_void_p]),
     "rgs_set_profiling": (C.c_int, [CTX, C.c_int]),
     "rgs_get_stage_times": (C.c_int, [CTX, FP, C.c_int]),

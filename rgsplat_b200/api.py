@@ -156,7 +156,7 @@ class Context:
         if rc != L.RGS_OK:
             raise RgsError(rc, "rgs_create failed")
         self.handle = h
-        self.options = o
+        self.create_options = o
 
     def check(self, rc: int) -> None:
         if rc != L.RGS_OK:
@@ -191,6 +191,15 @@ class Context:
         s = L.rgs_stats()
         self.check(self.lib.rgs_get_stats(self.handle, C.byref(s)))
         return {name: getattr(s, name) for name, _ in L.rgs_stats._fields_}
+
+    def options(self) -> dict:
+        o = L.rgs_options()
+        self.check(self.lib.rgs_get_options(self.handle, C.byref(o)))
+        return {name: getattr(o, name) for name, _ in L.rgs_options._fields_}
+
+    def set_tiling(self, tile: tuple[int, int], batch: int, pixels_per_thread: int) -> None:
+        """Blend-kernel layout (results are identical for every layout)."""
+        self.check(self.lib.rgs_set_tiling(self.handle, int(tile[0]), int(tile[1]), int(batch), int(pixels_per_thread)))
 
 
 _tls = threading.local()
@@ -244,6 +253,29 @@ def render_and_backward(gaussians, camera: Camera, target_rgba, bg=(0.0, 0.0, 0.
     lc = (cfg or LossConfig()).to_c()
     ctx.check(ctx.lib.rgs_render_and_backward(ctx.handle, _fp(g), n, C.byref(cam), _fp(tgt), _fp(bgv), C.byref(lc), C.byref(loss), _fp(grads)))
     return float(loss.value), grads
+
+
+def render_and_backward_variant(gaussians, camera: Camera, target_rgba, store_all: bool, bg=(0.0, 0.0, 0.0),
+                                cfg: LossConfig | None = None, ctx: Context | None = None):
+    """render_and_backward with the recompute-from-final-T backward (the
+    library's path) or the store-all-T variant -> (loss, grads, report) where
+    report holds the blend kernel times (ms) and the blend-state bytes."""
+    ctx = ctx or default_context()
+    g = _gauss(gaussians)
+    n = g.shape[0]
+    tgt = _f32(target_rgba).reshape(-1)
+    if tgt.size != camera.width * camera.height * 4:
+        raise ValueError("target must be w*h*4 RGBA floats")
+    grads = np.zeros((n, GRAD_FLOATS), np.float32)
+    loss = C.c_float(0.0)
+    cam = camera_c(camera)
+    lc = (cfg or LossConfig()).to_c()
+    rep = L.rgs_backward_report()
+    variant = L.RGS_BACKWARD_STORE_ALL if store_all else L.RGS_BACKWARD_RECOMPUTE
+    ctx.check(ctx.lib.rgs_render_and_backward_variant(ctx.handle, _fp(g), n, C.byref(cam), _fp(tgt), _fp(_f32(bg)), C.byref(lc),
+                                                      variant, C.byref(loss), _fp(grads), C.byref(rep)))
+    report = {name: getattr(rep, name) for name, _ in L.rgs_backward_report._fields_}
+    return float(loss.value), grads, report
 
 
 def render_color(gaussians, camera: Camera, bg=(0.0, 0.0, 0.0), ctx: Context | None = None) -> np.ndarray:
@@ -409,6 +441,22 @@ class Trainer:
                                                  C.byref(tc), int(mode), _fp(losses)))
         return losses[: v.size]
 
+    def step_host_targets(self, views: Sequence[int], target_ptrs: Sequence[int], bg=(0.0, 0.0, 0.0),
+                          loss_cfg: LossConfig | None = None, train_cfg: TrainConfig | None = None) -> np.ndarray:
+        """Batched step whose RGBA targets come from host memory (raw pointers,
+        one w*h*4 float32 image per view, page-locked for overlap); the copies
+        overlap the step's projection, sort and forward."""
+        v = np.ascontiguousarray(views, dtype=np.uint32)
+        if len(target_ptrs) != v.size:
+            raise ValueError("one target pointer per view")
+        ptrs = (C.c_void_p * max(v.size, 1))(*[int(p) for p in target_ptrs])
+        losses = np.zeros(max(v.size, 1), np.float32)
+        lc = (loss_cfg or LossConfig()).to_c()
+        tc = (train_cfg or TrainConfig()).to_c()
+        self.ctx.check(self.lib.rgs_trainer_step_host_targets(self.ctx.handle, v.ctypes.data_as(L.U32P), v.size, ptrs,
+                                                              _fp(_f32(bg)), C.byref(lc), C.byref(tc), _fp(losses)))
+        return losses[: v.size]
+
     def backward(self, views: Sequence[int], bg=(0.0, 0.0, 0.0), loss_cfg: LossConfig | None = None,
                  mode: int = L.RGS_STEP_PLAIN) -> np.ndarray:
         v = np.ascontiguousarray(views, dtype=np.uint32)
@@ -417,6 +465,24 @@ class Trainer:
         self.ctx.check(self.lib.rgs_trainer_backward(self.ctx.handle, v.ctypes.data_as(L.U32P), v.size, _fp(_f32(bg)), C.byref(lc),
                                                      int(mode), _fp(losses)))
         return losses[: v.size]
+
+    def autotune(self, views: Sequence[int], bg=(0.0, 0.0, 0.0), loss_cfg: LossConfig | None = None,
+                 reps: int = 3) -> tuple[dict, list[dict]]:
+        """Times every blend layout (tile 16x16 / 8x32 / 32x8 x batch 128 / 256 /
+        512 x 1 or 2 pixels per thread) on a batched render + backward of
+        ``views`` and keeps the fastest. Returns (chosen, all measurements).
+        Parameters and the Adam state are not modified."""
+        v = np.ascontiguousarray(views, dtype=np.uint32)
+        lc = (loss_cfg or LossConfig()).to_c()
+        res = (L.rgs_tune_entry * L.RGS_TUNE_CANDIDATES)()
+        chosen = L.rgs_options()
+        self.ctx.check(self.lib.rgs_trainer_autotune(self.ctx.handle, v.ctypes.data_as(L.U32P), v.size, _fp(_f32(bg)),
+                                                     C.byref(lc), int(reps), res, C.byref(chosen)))
+        table = [{"tile": f"{e.tile_w}x{e.tile_h}", "batch": e.batch, "pixels_per_thread": e.pixels_per_thread,
+                  "ms": round(float(e.ms), 4)} for e in res]
+        pick = {"tile": f"{chosen.tile_w}x{chosen.tile_h}", "batch": chosen.batch,
+                "pixels_per_thread": chosen.pixels_per_thread}
+        return pick, table
 
     def grads(self) -> np.ndarray:
         out = np.zeros((max(len(self), 1), GRAD_FLOATS), np.float32)

@@ -20,6 +20,10 @@ namespace rgs {
 
 constexpr int BIN_THREADS = 256;
 constexpr int BIN_SUB = 1024;  // ranks per emit sub-tile
+constexpr int EMIT_VT = 8;     // consecutive pairs per thread per emit round
+// staged-pair index with one pad word per 32, so a warp writing EMIT_VT-strided
+// words hits 32 distinct banks
+__device__ __forceinline__ int emit_pad(int i) { return i + (i >> 5); }
 
 int bin_grid_blocks() {
     static int g = 0;
@@ -101,6 +105,8 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit(const uint32_t* __restrict
     __shared__ uint32_t s_slot[BIN_SUB];
     __shared__ uint2 s_desc[BIN_SUB];  // (first tile id, rect width | view tiles_x << 16)
     __shared__ uint32_t s_w[BIN_THREADS / 32];
+    __shared__ uint32_t s_ek[BIN_THREADS * EMIT_VT + BIN_THREADS * EMIT_VT / 32];
+    __shared__ uint32_t s_ev[BIN_THREADS * EMIT_VT + BIN_THREADS * EMIT_VT / 32];
     constexpr int PER = BIN_SUB / BIN_THREADS;
     int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     uint32_t begin, end;
@@ -143,28 +149,62 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit(const uint32_t* __restrict
         }
         if (tid == 0) s_off[BIN_SUB] = sub_total;
         __syncthreads();
-        for (uint32_t q = tid; q < sub_total; q += BIN_THREADS) {
-            // largest r with s_off[r] <= q (that entry has a non-zero count)
-            int lo = 0, hi = BIN_SUB - 1;
-            while (lo < hi) {
-                int mid = (lo + hi + 1) >> 1;
-                if (s_off[mid] <= q) lo = mid;
-                else hi = mid - 1;
+        // Expansion in rounds of BIN_THREADS * EMIT_VT outputs: every thread
+        // produces EMIT_VT consecutive pairs (one binary search for the first,
+        // then a walk along the rectangles), stages them in shared memory, and
+        // the block writes the round out with consecutive threads on
+        // consecutive addresses.
+        for (uint32_t o0 = 0; o0 < sub_total; o0 += BIN_THREADS * EMIT_VT) {
+            const uint32_t qb = o0 + (uint32_t)(tid * EMIT_VT);
+            if (qb < sub_total) {
+                // largest r with s_off[r] <= qb (that entry has a non-zero count)
+                int lo = 0, hi = BIN_SUB - 1;
+                while (lo < hi) {
+                    int mid = (lo + hi + 1) >> 1;
+                    if (s_off[mid] <= qb) lo = mid;
+                    else hi = mid - 1;
+                }
+                int r = lo;
+                uint2 d = s_desc[r];
+                uint32_t wt = d.y & 0xffffu;
+                uint32_t j = qb - s_off[r];
+                uint32_t row = j / wt, col = j - row * wt;
+                uint32_t next = s_off[r + 1];
+#pragma unroll
+                for (int k = 0; k < EMIT_VT; ++k) {
+                    const uint32_t q = qb + (uint32_t)k;
+                    if (q >= sub_total) break;
+                    while (q >= next) {  // next rectangle with a non-zero count
+                        ++r;
+                        next = s_off[r + 1];
+                        d = s_desc[r];
+                        wt = d.y & 0xffffu;
+                        row = 0;
+                        col = 0;
+                    }
+                    // tile ids of one view are row-major: row `row` of the
+                    // rectangle starts row * tiles_x after its first tile
+                    const int sp = emit_pad(tid * EMIT_VT + k);
+                    s_ek[sp] = d.x + row * (d.y >> 16) + col;
+                    s_ev[sp] = s_slot[r];
+                    if (++col == wt) {
+                        col = 0;
+                        ++row;
+                    }
+                }
             }
-            const uint2 d = s_desc[lo];
-            const uint32_t j = q - s_off[lo];
-            const uint32_t wt = d.y & 0xffffu;
-            const uint32_t row = j / wt;
-            // tile ids of one view are row-major: row r of the rectangle starts
-            // r * tiles_x after its first tile
-            const uint32_t key = d.x + row * (d.y >> 16) + (j - row * wt);
-            uint32_t out = base + q;
-            if (out < cap) {
-                pkeys[out] = key;
-                pvals[out] = s_slot[lo];
-            } else {
-                *overflow = 1;
+            __syncthreads();
+            const uint32_t n_round = min((uint32_t)(BIN_THREADS * EMIT_VT), sub_total - o0);
+            for (uint32_t i = tid; i < n_round; i += BIN_THREADS) {
+                const uint32_t out = base + o0 + i;
+                if (out < cap) {
+                    pkeys[out] = s_ek[emit_pad((int)i)];
+                    pvals[out] = s_ev[emit_pad((int)i)];
+                } else {
+                    *overflow = 1;
+                }
             }
+            __syncthreads();
         }
         base += sub_total;
         __syncthreads();
@@ -178,13 +218,44 @@ void launch_emit_pairs(const uint32_t* order, const uint2* tdesc, uint32_t S, co
                                          n_per_view);
 }
 
-__global__ void k_tile_ranges(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ total, uint32_t cap,
-                              uint2* __restrict__ ranges) {
-    uint32_t K = min(*total, cap);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < K; i += gridDim.x * blockDim.x) {
-        uint32_t t = keys[i];
-        if (i == 0 || keys[i - 1] != t) ranges[t].x = i;
-        if (i == K - 1 || keys[i + 1] != t) ranges[t].y = i + 1;
+// Tile boundaries of the sorted pair keys: each thread takes four consecutive
+// keys with one 16-byte load (the key buffers are 256-byte aligned), its
+// neighbours' edge keys come from the adjacent lanes (or memory at warp
+// edges).
+__global__ void __launch_bounds__(256) k_tile_ranges(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ total,
+                                                     uint32_t cap, uint2* __restrict__ ranges) {
+    const uint32_t K = min(*total, cap);
+    const uint32_t nq = (K + 3u) / 4u;
+    const int lane = threadIdx.x & 31;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    // uniform trip count per warp so the shuffles see every lane
+    for (uint32_t q0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); q0 < nq; q0 += stride) {
+        const uint32_t q = q0 + (uint32_t)lane;
+        const uint32_t i = q * 4u;
+        uint32_t k[4];
+        if (i + 3u < K) {
+            const uint4 v = *reinterpret_cast<const uint4*>(keys + i);
+            k[0] = v.x; k[1] = v.y; k[2] = v.z; k[3] = v.w;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) k[j] = i + (uint32_t)j < K ? keys[i + j] : 0xffffffffu;
+        }
+        uint32_t prev = __shfl_up_sync(0xffffffffu, k[3], 1);
+        uint32_t next = __shfl_down_sync(0xffffffffu, k[0], 1);
+        if (lane == 0 && i > 0 && i < K) prev = keys[i - 1];
+        if (lane == 31 && i + 4u < K) next = keys[i + 4u];
+        if (i < K) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t p = i + (uint32_t)j;
+                if (p >= K) break;
+                const uint32_t t = k[j];
+                const uint32_t before = j == 0 ? prev : k[j - 1];
+                const uint32_t after = j == 3 ? next : k[j + 1];
+                if (p == 0 || before != t) ranges[t].x = p;
+                if (p == K - 1 || after != t) ranges[t].y = p + 1;
+            }
+        }
     }
 }
 

@@ -134,7 +134,7 @@ __device__ __forceinline__ int stage_batch(const BlendArgs& a, size_t S, uint32_
 // Forward. PPT vertically adjacent pixels per thread share dx and the
 // dx-only products of power, which are evaluated once per (splat, thread) in
 // the reference's rounding order.
-template <int TW, int TH, int BATCH, bool RECT, int PPT>
+template <int TW, int TH, int BATCH, bool RECT, int PPT, bool STORE = false>
 __global__ void __launch_bounds__(TW * TH / PPT) k_blend_fwd(BlendArgs a) {
     constexpr int NT = TW * TH / PPT;
     __shared__ float4 s_a[BATCH];
@@ -162,12 +162,13 @@ __global__ void __launch_bounds__(TW * TH / PPT) k_blend_fwd(BlendArgs a) {
         const float x0c = (float)(tx * TW) + 0.5f, x1c = (float)(min(tx * TW + TW, c.width) - 1) + 0.5f;
         const float y0c = (float)(ty * TH) + 0.5f, y1c = (float)(min(ty * TH + TH, c.height) - 1) + 0.5f;
         const uint2 rg = a.ranges[tile];
-        float T[PPT], C0[PPT], C1[PPT], C2[PPT];
+        float T[PPT], C0[PPT], C1[PPT], C2[PPT], pyc[PPT];
         int last[PPT];
         bool done[PPT], seen[PPT];
         bool all_done = true;
 #pragma unroll
         for (int p = 0; p < PPT; ++p) {
+            pyc[p] = (float)(py0 + p) + 0.5f;
             T[p] = 1.0f;
             C0[p] = C1[p] = C2[p] = 0.0f;
             last[p] = -1;
@@ -200,12 +201,13 @@ __global__ void __launch_bounds__(TW * TH / PPT) k_blend_fwd(BlendArgs a) {
                 for (int p = 0; p < PPT; ++p) {
                     if (done[p]) continue;
                     if (RECT && !in_rect(Q.w, s_k[k].w, px, py0 + p)) continue;
-                    const float dy = ((float)(py0 + p) + 0.5f) - A.y;
+                    const float dy = pyc[p] - A.y;
                     const float power = -0.5f * (tdx + t2b * dy + Q.z * dy * dy);
                     if (power > 0.0f || power < A.w) continue;
-                    const float alpha = fminf(A.z * expf_fast(power), 0.99f);
+                    const float alpha = fminf(A.z * expf_fast_nonpos(power), 0.99f);
                     if (alpha < 1.0f / 255.0f) continue;
                     const float4 K = s_k[k];
+                    if (STORE) a.tstore[(size_t)(rg.x + (uint32_t)s_li[k]) * (TW * TH) + (tid / TW) * PPT * TW + p * TW + tid % TW] = T[p];
                     const float weight = alpha * T[p];
                     C0[p] += K.x * weight;
                     C1[p] += K.y * weight;
@@ -281,7 +283,7 @@ __device__ __forceinline__ void red_add_v4(float4* addr, float x, float y, float
 // a splat are summed in registers before the warp reduction. T is rebuilt as
 // T * 1/(1 - alpha) (one correctly rounded reciprocal serves both uses; the
 // reference divides, backward.rs:452, which differs by an ulp).
-template <int TW, int TH, int BATCH, bool RECT, int PPT>
+template <int TW, int TH, int BATCH, bool RECT, int PPT, bool STORE = false>
 __global__ void __launch_bounds__(TW * TH / PPT) k_blend_bwd(BlendArgs a) {
     constexpr int NT = TW * TH / PPT;
     constexpr int NACC = 9;
@@ -315,11 +317,12 @@ __global__ void __launch_bounds__(TW * TH / PPT) k_blend_bwd(BlendArgs a) {
         const float y0c = (float)(ty * TH) + 0.5f, y1c = (float)(min(ty * TH + TH, c.height) - 1) + 0.5f;
         const uint2 rg = a.ranges[tile];
         int lc[PPT];
-        float T[PPT], dl0[PPT], dl1[PPT], dl2[PPT], be0[PPT], be1[PPT], be2[PPT];
+        float T[PPT], dl0[PPT], dl1[PPT], dl2[PPT], be0[PPT], be1[PPT], be2[PPT], pyc[PPT];
         int my_maxlc = -1;
 #pragma unroll
         for (int p = 0; p < PPT; ++p) {
             const int py = py0 + p;
+            pyc[p] = (float)py + 0.5f;
             lc[p] = -1;
             T[p] = 0.0f;
             dl0[p] = dl1[p] = dl2[p] = 0.0f;
@@ -363,38 +366,48 @@ __global__ void __launch_bounds__(TW * TH / PPT) k_blend_bwd(BlendArgs a) {
                     const float dx = pxf - A.x;
                     const float tdx = Q.x * dx * dx;
                     const float t2b = 2.0f * Q.y * dx;
+                    // per-entry factors of the conic / mean gradients
+                    const float hdxx = -0.5f * dx * dx, qxdx = Q.x * dx, qydx = Q.y * dx;
 #pragma unroll
                     for (int p = 0; p < PPT; ++p) {
                         if (li > lc[p]) continue;
                         if (RECT && !in_rect(Q.w, K.w, px, py0 + p)) continue;
-                        const float dy = ((float)(py0 + p) + 0.5f) - A.y;
+                        // alpha exactly as the forward computed it
+                        const float dy = pyc[p] - A.y;
                         const float power = -0.5f * (tdx + t2b * dy + Q.z * dy * dy);
                         if (power > 0.0f || power < A.w) continue;
-                        const float g_exp = expf_fast(power);
+                        const float g_exp = expf_fast_nonpos(power);
                         const float alpha_raw = A.z * g_exp;
                         const float alpha = fminf(alpha_raw, 0.99f);
                         if (alpha < 1.0f / 255.0f) continue;
-                        const float inv_1ma = __frcp_rn(1.0f - alpha);
-                        T[p] = T[p] * inv_1ma;
+                        float inv_1ma;
+                        if (STORE) {
+                            // store-all variant: T before this splat as the forward saw it
+                            T[p] = a.tstore[(size_t)(rg.x + (uint32_t)li) * (TW * TH) + (tid / TW) * PPT * TW + p * TW + tid % TW];
+                            inv_1ma = 1.0f / (1.0f - alpha);
+                        } else {
+                            inv_1ma = __frcp_rn(1.0f - alpha);
+                            T[p] = T[p] * inv_1ma;
+                        }
+                        // gradient terms of backward.rs:453-484, as fused multiply-adds
                         const float weight = alpha * T[p];
-                        g[0] += dl0[p] * weight;
-                        g[1] += dl1[p] * weight;
-                        g[2] += dl2[p] * weight;
-                        float dl_dalpha = 0.0f;
-                        dl_dalpha += dl0[p] * (T[p] * K.x - be0[p] * inv_1ma);
-                        dl_dalpha += dl1[p] * (T[p] * K.y - be1[p] * inv_1ma);
-                        dl_dalpha += dl2[p] * (T[p] * K.z - be2[p] * inv_1ma);
-                        const float dl_draw = dl_dalpha * (alpha_raw > 0.99f ? 0.0f : 1.0f);
-                        g[3] += dl_draw * g_exp;
+                        g[0] = __fmaf_rn(dl0[p], weight, g[0]);
+                        g[1] = __fmaf_rn(dl1[p], weight, g[1]);
+                        g[2] = __fmaf_rn(dl2[p], weight, g[2]);
+                        float dl_dalpha = dl0[p] * __fmaf_rn(T[p], K.x, -be0[p] * inv_1ma);
+                        dl_dalpha = __fmaf_rn(dl1[p], __fmaf_rn(T[p], K.y, -be1[p] * inv_1ma), dl_dalpha);
+                        dl_dalpha = __fmaf_rn(dl2[p], __fmaf_rn(T[p], K.z, -be2[p] * inv_1ma), dl_dalpha);
+                        const float dl_draw = alpha_raw > 0.99f ? 0.0f : dl_dalpha;
+                        g[3] = __fmaf_rn(dl_draw, g_exp, g[3]);
                         const float dl_dpower = dl_draw * A.z * g_exp;
-                        g[4] += dl_dpower * (-0.5f * dx * dx);
-                        g[5] += dl_dpower * (-dx * dy);
-                        g[6] += dl_dpower * (-0.5f * dy * dy);
-                        g[7] += dl_dpower * (Q.x * dx + Q.y * dy);
-                        g[8] += dl_dpower * (Q.y * dx + Q.z * dy);
-                        be0[p] += weight * K.x;
-                        be1[p] += weight * K.y;
-                        be2[p] += weight * K.z;
+                        g[4] = __fmaf_rn(dl_dpower, hdxx, g[4]);
+                        g[5] = __fmaf_rn(dl_dpower, -dx * dy, g[5]);
+                        g[6] = __fmaf_rn(dl_dpower, -0.5f * dy * dy, g[6]);
+                        g[7] = __fmaf_rn(dl_dpower, __fmaf_rn(Q.y, dy, qxdx), g[7]);
+                        g[8] = __fmaf_rn(dl_dpower, __fmaf_rn(Q.z, dy, qydx), g[8]);
+                        be0[p] = __fmaf_rn(weight, K.x, be0[p]);
+                        be1[p] = __fmaf_rn(weight, K.y, be1[p]);
+                        be2[p] = __fmaf_rn(weight, K.z, be2[p]);
                         contrib = true;
                     }
                 }
@@ -483,5 +496,17 @@ static void launch(const BlendArgs& a, int tw, int th, int batch, bool fwd, cuda
 
 void launch_blend_forward(const BlendArgs& a, int tw, int th, int batch, cudaStream_t st) { launch(a, tw, th, batch, true, st); }
 void launch_blend_backward(const BlendArgs& a, int tw, int th, int batch, cudaStream_t st) { launch(a, tw, th, batch, false, st); }
+
+// Store-all variant (16x16 tiles, 256-splat batches, 2 pixels per thread): the
+// forward writes T before every contributing splat of every pixel to
+// a.tstore[(list position) * 256 + pixel in tile], the backward reads it back
+// instead of rebuilding T from the final T.
+void launch_blend_store_all(const BlendArgs& a, bool fwd, cudaStream_t st) {
+    BlendKernel k = fwd ? (BlendKernel)k_blend_fwd<16, 16, 256, false, 2, true> : (BlendKernel)k_blend_bwd<16, 16, 256, false, 2, true>;
+    cudaMemsetAsync(a.work, 0, sizeof(uint32_t), st);
+    int grid = grid_for(k, 128);
+    if (!a.total_tiles) grid = std::min(grid, std::max(a.total_tiles_host, 1));
+    k<<<grid, 128, 0, st>>>(a);
+}
 
 }  // namespace rgs

@@ -80,11 +80,16 @@ struct rgs_ctx {
     SortScratch sort;
     DBuf dens_scratch, dens_out, m_tmp;
     DBuf stage_a, stage_b, stage_c, stage_d, target_stage;
+    DBuf tstore;  // store-all backward study only
     // batched-step graph
     cudaGraphExec_t gexec = nullptr;
     std::vector<uint64_t> g_key;
     rgs_stats stats{};
     cudaStream_t own_stream = nullptr;
+    // host-target steps: targets copied on copy_st, the loss waits on ev_copy
+    cudaStream_t copy_st = nullptr;
+    cudaEvent_t ev_copy = nullptr;
+    DBuf target_batch;
     // per-stage timing (boundaries 0..RGS_NUM_STAGES)
     bool prof = false;
     cudaEvent_t ev[RGS_NUM_STAGES + 1] = {};
@@ -455,6 +460,7 @@ BlendArgs blend_args(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, cons
     a.rect_filter = 0;
     a.empty_tile_black = 1;
     a.pixels_per_thread = ctx->opt.pixels_per_thread;
+    a.tstore = nullptr;
     return a;
 }
 
@@ -471,10 +477,18 @@ int upload_single_cam(rgs_ctx* ctx, const DevCam& d, DevCam** dev) {
     return RGS_OK;
 }
 
+// Differentiation study (rgs_render_and_backward_variant): which backward,
+// and the blend-kernel times and blend-state bytes it measured.
+struct BwdStudy {
+    bool store_all = false;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    uint64_t state_bytes = 0;
+};
+
 // Forward + loss + backward + geometry of one view (the plain path).
 // grads: accumulate (v > 0) or overwrite into s.grads; loss_out may be null.
 int run_view_plain(rgs_ctx* ctx, Scene& s, const DevCam& dc_in, const float* target_dev, const float bg[3], float lambda,
-                   bool do_backward, bool accumulate, float* loss_out, float* rgb_host) {
+                   bool do_backward, bool accumulate, float* loss_out, float* rgb_host, BwdStudy* study = nullptr) {
     cudaStream_t st = ctx->st;
     DevCam dc = dc_in;
     dc.target = target_dev;
@@ -488,7 +502,23 @@ int run_view_plain(rgs_ctx* ctx, Scene& s, const DevCam& dc_in, const float* tar
     Binned b;
     if ((rc = bin_batch(ctx, s, cams_dev, 1, tiles, true, b))) return rc;
     BlendArgs fa = blend_args(ctx, s, cams_dev, 1, nullptr, tiles, b, bg, true);
-    launch_blend_forward(fa, ctx->opt.tile_w, ctx->opt.tile_h, ctx->opt.batch, st);
+    if (study) {
+        // blend state: final T + last contributor per pixel, plus (store-all)
+        // T per (tile-list position, tile pixel)
+        study->state_bytes = (uint64_t)px * 8;
+        if (study->store_all) {
+            const uint64_t need = (uint64_t)ctx->stats.pairs * (uint64_t)(REF_TILE * REF_TILE) * 4;
+            CK(ctx->tstore.ensure(std::max<uint64_t>(need, 16)));
+            study->state_bytes += need;
+            fa.tstore = ctx->tstore.as<float>();
+        }
+        CK(cudaEventRecord(study->ev[0], st));
+        if (study->store_all) launch_blend_store_all(fa, true, st);
+        else launch_blend_forward(fa, ctx->opt.tile_w, ctx->opt.tile_h, ctx->opt.batch, st);
+        CK(cudaEventRecord(study->ev[1], st));
+    } else {
+        launch_blend_forward(fa, ctx->opt.tile_w, ctx->opt.tile_h, ctx->opt.batch, st);
+    }
     mark(ctx, 6);
     CK(cudaGetLastError());
     if (rgb_host) {
@@ -502,7 +532,15 @@ int run_view_plain(rgs_ctx* ctx, Scene& s, const DevCam& dc_in, const float* tar
     mark(ctx, 7);
     CK(cudaMemsetAsync(ctx->acc.p, 0, std::max<size_t>(s.n, 1) * 3 * sizeof(float4), st));
     BlendArgs ba = blend_args(ctx, s, cams_dev, 1, nullptr, tiles, b, bg, false);
-    launch_blend_backward(ba, ctx->opt.tile_w, ctx->opt.tile_h, ctx->opt.batch, st);
+    if (study) {
+        ba.tstore = fa.tstore;
+        CK(cudaEventRecord(study->ev[2], st));
+        if (study->store_all) launch_blend_store_all(ba, false, st);
+        else launch_blend_backward(ba, ctx->opt.tile_w, ctx->opt.tile_h, ctx->opt.batch, st);
+        CK(cudaEventRecord(study->ev[3], st));
+    } else {
+        launch_blend_backward(ba, ctx->opt.tile_w, ctx->opt.tile_h, ctx->opt.batch, st);
+    }
     mark(ctx, 8);
     launch_geometry(s.params.as<float4>(), s.n, s.cap, cams_dev, 1, ctx->cnt.as<uint32_t>(), ctx->acc.as<float4>(),
                     ctx->rec.as<float4>(), ctx->gv.as<float4>(), s.grads.as<float4>(), accumulate ? 1 : 0, st);
@@ -599,7 +637,7 @@ int rgs_create(const rgs_options* opts, rgs_ctx** out) {
     }
     std::memset(ctx->hdr_h, 0, sizeof(StepHdr));
     std::memset(ctx->out_h, 0, sizeof(StepOut));
-    ctx->sort_grid = ctx->sms * 2;
+    ctx->sort_grid = sort_grid_blocks();
     *out = ctx;
     return RGS_OK;
 }
@@ -618,12 +656,16 @@ void rgs_destroy(rgs_ctx* ctx) {
                     &ctx->ranges, &ctx->rgb, &ctx->final_t, &ctx->last, &ctx->dl, &ctx->partials, &ctx->scalars,
                     &ctx->block_sums, &ctx->sort.hist, &ctx->sort.keys2, &ctx->sort.vals2, &ctx->dens_scratch,
                     &ctx->dens_out, &ctx->m_tmp, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->stage_d,
-                    &ctx->target_stage};
+                    &ctx->target_stage, &ctx->tstore};
     for (DBuf* b : bufs) b->release();
     if (ctx->hdr_h) cudaFreeHost(ctx->hdr_h);
     if (ctx->out_h) cudaFreeHost(ctx->out_h);
     for (int i = 0; i <= RGS_NUM_STAGES; ++i)
         if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+    if (ctx->copy_st) cudaStreamSynchronize(ctx->copy_st);
+    ctx->target_batch.release();
+    if (ctx->ev_copy) cudaEventDestroy(ctx->ev_copy);
+    if (ctx->copy_st) cudaStreamDestroy(ctx->copy_st);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
 }
@@ -691,6 +733,54 @@ int rgs_render_and_backward(rgs_ctx* ctx, const float* gaussians, size_t n, cons
     if ((rc = run_view_plain(ctx, s, dc, ctx->target_stage.as<float>(), bg, cfg->lambda_dssim, true, false, &loss, nullptr)))
         return rc;
     if (loss_out) *loss_out = loss;
+    if (grads_out && n) {
+        CK(ctx->stage_b.ensure(n * NG * 4));
+        launch_grads_to_aos(s.grads.as<float4>(), ctx->stage_b.as<float>(), (int)n, s.cap, NG, ctx->st);
+        CK(cudaMemcpyAsync(grads_out, ctx->stage_b.p, n * NG * 4, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+    }
+    return RGS_OK;
+}
+
+int rgs_render_and_backward_variant(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera,
+                                    const float* target_rgba, const float bg[3], const rgs_loss_config* cfg, int variant,
+                                    float* loss_out, float* grads_out, rgs_backward_report* report) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!camera || !target_rgba || !bg || !cfg || (n && !gaussians)) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
+    if (variant != RGS_BACKWARD_RECOMPUTE && variant != RGS_BACKWARD_STORE_ALL)
+        return fail(ctx, RGS_ERR_INVALID_ARG, "unknown backward variant");
+    if (variant == RGS_BACKWARD_STORE_ALL && !(ctx->opt.tile_w == REF_TILE && ctx->opt.tile_h == REF_TILE))
+        return fail(ctx, RGS_ERR_INVALID_ARG, "the store-all backward needs 16x16 tiles");
+    DevCam dc;
+    if ((rc = make_devcam(ctx, *camera, dc))) return rc;
+    Scene& s = ctx->sc;
+    if ((rc = upload_gaussians(ctx, s, gaussians, n))) return rc;
+    if ((rc = check_finite(ctx, s))) return rc;
+    size_t px = (size_t)camera->width * camera->height;
+    CK(ctx->target_stage.ensure(px * 4 * 4));
+    CK(cudaMemcpyAsync(ctx->target_stage.p, target_rgba, px * 16, cudaMemcpyHostToDevice, ctx->st));
+    ctx->stats = rgs_stats{};
+    BwdStudy study;
+    study.store_all = variant == RGS_BACKWARD_STORE_ALL;
+    for (auto& e : study.ev) CK(cudaEventCreate(&e));
+    float loss = 0.0f;
+    rc = run_view_plain(ctx, s, dc, ctx->target_stage.as<float>(), bg, cfg->lambda_dssim, true, false, &loss, nullptr, &study);
+    float fwd_ms = 0.0f, bwd_ms = 0.0f;
+    if (rc == RGS_OK) {
+        cudaError_t e = cudaEventElapsedTime(&fwd_ms, study.ev[0], study.ev[1]);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&bwd_ms, study.ev[2], study.ev[3]);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "variant timing");
+    }
+    for (auto& e : study.ev) cudaEventDestroy(e);
+    if (rc) return rc;
+    if (loss_out) *loss_out = loss;
+    if (report) {
+        report->forward_ms = fwd_ms;
+        report->backward_ms = bwd_ms;
+        report->state_bytes = study.state_bytes;
+        report->pairs = ctx->stats.pairs;
+    }
     if (grads_out && n) {
         CK(ctx->stage_b.ensure(n * NG * 4));
         launch_grads_to_aos(s.grads.as<float4>(), ctx->stage_b.as<float>(), (int)n, s.cap, NG, ctx->st);
@@ -1021,7 +1111,7 @@ void batch_caps(rgs_ctx* ctx, int V, size_t& px, size_t& tiles, size_t& lb) {
 }
 
 int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], float lambda, const rgs_train_config& tc,
-                    bool fused) {
+                    bool fused, bool host_targets) {
     Scene& s = ctx->tr;
     cudaStream_t st = ctx->st;
     if (ctx->gexec) {
@@ -1046,6 +1136,9 @@ int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], fl
         BlendArgs fa = blend_args(ctx, s, cams_dev, V, &hd->total_tiles, tiles_cap, b, bg, true);
         launch_blend_forward(fa, ctx->opt.tile_w, ctx->opt.tile_h, ctx->opt.batch, st);
         mark(ctx, 6);
+        // the step's targets were copied from host memory on copy_st, issued
+        // just before this graph's launch; only the loss waits for them
+        if (host_targets) cudaStreamWaitEvent(st, ctx->ev_copy, cudaEventWaitExternal);
         launch_loss(cams_dev, V, 0, ctx->rgb.as<float>(), lambda, ctx->dl.as<float>(), ctx->partials.as<float>(), losses_dev,
                     &hd->total_loss_blocks, st);
         mark(ctx, 7);
@@ -1087,7 +1180,7 @@ int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], fl
 // Batched path: one launch per stage over all views, replayed from a CUDA
 // graph; the fused geometry-backward + Adam kernel ends the step.
 int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], float lambda, const rgs_train_config& tc,
-                 float* losses, bool fused) {
+                 float* losses, bool fused, const float* const* host_targets = nullptr) {
     Scene& s = ctx->tr;
     StepHdr* h = ctx->hdr_h;
     for (int v = 0; v < V; ++v) {
@@ -1106,6 +1199,16 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
     if (rc) return rc;
     if (!ctx->pkeys.p && (rc = ensure_pairs(ctx, S * 4))) return rc;
     if ((rc = ensure_moments(ctx, s, s.n))) return rc;
+    if (host_targets) {
+        if (!ctx->copy_st) {
+            CK(cudaStreamCreateWithFlags(&ctx->copy_st, cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&ctx->ev_copy, cudaEventDisableTiming));
+        }
+        // the previous step has finished (it synchronised), so the batch
+        // target buffer is free to refill
+        CK(ctx->target_batch.ensure(px_cap * 16));
+        for (int v = 0; v < V; ++v) h->cams[v].target = ctx->target_batch.as<float>() + (size_t)h->cams[v].pix_base * 4;
+    }
     const uint64_t tstep = fused ? 1 : 0;
     for (int attempt = 0; attempt < 4; ++attempt) {
         s.t += tstep;
@@ -1122,7 +1225,9 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
         auto make_key = [&]() {
             std::vector<uint64_t> key = {(uint64_t)s.n, (uint64_t)s.cap, (uint64_t)V, (uint64_t)s.mcap, ctx->pair_cap,
                                          px_cap, tiles_cap, lb_cap, (uint64_t)fused, (uint64_t)ctx->prof,
-                                         (uint64_t)(uintptr_t)ctx->st};
+                                         (uint64_t)(uintptr_t)ctx->st, (uint64_t)ctx->opt.tile_w,
+                                         (uint64_t)ctx->opt.tile_h, (uint64_t)ctx->opt.batch,
+                                         (uint64_t)ctx->opt.pixels_per_thread, (uint64_t)(host_targets != nullptr)};
             for (const DBuf* b : bufs) key.push_back((uint64_t)(uintptr_t)b->p);
             for (float f : fk) {
                 uint32_t u;
@@ -1134,12 +1239,18 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
         std::vector<uint64_t> key = make_key();
         if (!ctx->gexec || key != ctx->g_key) {
             for (int i = 0; i <= RGS_NUM_STAGES; ++i) ctx->ev_marked[i] = false;
-            if ((rc = capture_batched(ctx, V, tiles_cap, bg, lambda, tc, fused))) {
+            if ((rc = capture_batched(ctx, V, tiles_cap, bg, lambda, tc, fused, host_targets != nullptr))) {
                 s.t -= tstep;
                 return rc;
             }
             for (int i = 0; i <= RGS_NUM_STAGES; ++i) ctx->graph_marked[i] = ctx->ev_marked[i];
             ctx->g_key = make_key();  // capture may have grown scratch buffers
+        }
+        if (host_targets && attempt == 0) {
+            for (int v = 0; v < V; ++v)
+                CK(cudaMemcpyAsync((void*)h->cams[v].target, host_targets[v],
+                                   (size_t)h->cams[v].width * h->cams[v].height * 16, cudaMemcpyHostToDevice, ctx->copy_st));
+            CK(cudaEventRecord(ctx->ev_copy, ctx->copy_st));
         }
         CK(cudaGraphLaunch(ctx->gexec, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
@@ -1182,6 +1293,18 @@ int rgs_trainer_step(rgs_ctx* ctx, const uint32_t* views, size_t nviews, const f
     return RGS_OK;
 }
 
+int rgs_trainer_step_host_targets(rgs_ctx* ctx, const uint32_t* views, size_t nviews, const float* const* targets_rgba,
+                                  const float bg[3], const rgs_loss_config* loss_cfg, const rgs_train_config* train_cfg,
+                                  float* losses_out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!bg || !loss_cfg || !train_cfg || !targets_rgba) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
+    if ((rc = check_views(ctx, views, nviews, false))) return rc;
+    for (size_t v = 0; v < nviews; ++v)
+        if (!targets_rgba[v]) return fail(ctx, RGS_ERR_INVALID_ARG, "null target pointer");
+    return batched_step(ctx, views, (int)nviews, bg, loss_cfg->lambda_dssim, *train_cfg, losses_out, true, targets_rgba);
+}
+
 int rgs_trainer_backward(rgs_ctx* ctx, const uint32_t* views, size_t nviews, const float bg[3], const rgs_loss_config* loss_cfg,
                          int mode, float* losses_out) {
     int rc = check_ctx(ctx);
@@ -1195,6 +1318,89 @@ int rgs_trainer_backward(rgs_ctx* ctx, const uint32_t* views, size_t nviews, con
     }
     if (mode != RGS_STEP_PLAIN) return fail(ctx, RGS_ERR_INVALID_ARG, "unknown step mode");
     return plain_backward(ctx, views, nviews, bg, loss_cfg->lambda_dssim, losses_out);
+}
+
+int rgs_get_options(rgs_ctx* ctx, rgs_options* out) {
+    if (!ctx || !out) return RGS_ERR_INVALID_ARG;
+    *out = ctx->opt;
+    return RGS_OK;
+}
+
+int rgs_set_tiling(rgs_ctx* ctx, int tile_w, int tile_h, int batch, int pixels_per_thread) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    bool shape_ok = (tile_w == 16 && tile_h == 16) || (tile_w == 8 && tile_h == 32) || (tile_w == 32 && tile_h == 8);
+    if (!shape_ok) return fail(ctx, RGS_ERR_INVALID_ARG, "tile shape must be 16x16, 8x32 or 32x8");
+    if (batch != 128 && batch != 256 && batch != 512) return fail(ctx, RGS_ERR_INVALID_ARG, "batch must be 128, 256 or 512");
+    if (pixels_per_thread != 1 && pixels_per_thread != 2)
+        return fail(ctx, RGS_ERR_INVALID_ARG, "pixels_per_thread must be 1 or 2");
+    // the graph key holds the layout, so the next batched step recaptures
+    ctx->opt.tile_w = tile_w;
+    ctx->opt.tile_h = tile_h;
+    ctx->opt.batch = batch;
+    ctx->opt.pixels_per_thread = pixels_per_thread;
+    return RGS_OK;
+}
+
+// Autotuner: every layout is timed on the same views with CUDA events on the
+// context's stream around `reps` batched render + backward passes (after one
+// untimed pass that captures the layout's graph and warms it), and the fastest
+// one is kept. Gradients are overwritten; parameters, moments, grad_accum /
+// grad_denom and the Adam step count are untouched (MODE 0 of the geometry
+// pass writes gradients only).
+int rgs_trainer_autotune(rgs_ctx* ctx, const uint32_t* views, size_t nviews, const float bg[3], const rgs_loss_config* loss_cfg,
+                         int reps, rgs_tune_entry* results, rgs_options* chosen) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!bg || !loss_cfg) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
+    if (reps < 1) return fail(ctx, RGS_ERR_INVALID_ARG, "reps must be >= 1");
+    if ((rc = check_views(ctx, views, nviews, true))) return rc;
+    static const int shapes[3][2] = {{16, 16}, {8, 32}, {32, 8}};
+    static const int batches[3] = {128, 256, 512};
+    rgs_train_config tc;
+    rgs_train_config_default(&tc);
+    const rgs_options saved = ctx->opt;
+    const bool prof = ctx->prof;
+    ctx->prof = false;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t ce = cudaEventCreate(&e0);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+    if (ce != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        ctx->prof = prof;
+        return cuda_fail(ctx, ce, "autotune events");
+    }
+    float best = 0.0f;
+    rgs_options best_opt = saved;
+    int k = 0;
+    for (int si = 0; si < 3 && rc == RGS_OK; ++si)
+        for (int bi = 0; bi < 3 && rc == RGS_OK; ++bi)
+            for (int ppt = 1; ppt <= 2 && rc == RGS_OK; ++ppt, ++k) {
+                ctx->opt.tile_w = shapes[si][0];
+                ctx->opt.tile_h = shapes[si][1];
+                ctx->opt.batch = batches[bi];
+                ctx->opt.pixels_per_thread = ppt;
+                rc = batched_step(ctx, views, (int)nviews, bg, loss_cfg->lambda_dssim, tc, nullptr, false);
+                float ms = 0.0f;
+                if (rc == RGS_OK && (ce = cudaEventRecord(e0, ctx->st)) != cudaSuccess) rc = cuda_fail(ctx, ce, "autotune");
+                for (int r = 0; r < reps && rc == RGS_OK; ++r)
+                    rc = batched_step(ctx, views, (int)nviews, bg, loss_cfg->lambda_dssim, tc, nullptr, false);
+                if (rc == RGS_OK && (ce = cudaEventRecord(e1, ctx->st)) != cudaSuccess) rc = cuda_fail(ctx, ce, "autotune");
+                if (rc == RGS_OK && (ce = cudaEventSynchronize(e1)) != cudaSuccess) rc = cuda_fail(ctx, ce, "autotune");
+                if (rc == RGS_OK && (ce = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) rc = cuda_fail(ctx, ce, "autotune");
+                ms /= (float)reps;
+                if (results) results[k] = rgs_tune_entry{shapes[si][0], shapes[si][1], batches[bi], ppt, ms};
+                if (rc == RGS_OK && (k == 0 || ms < best)) {
+                    best = ms;
+                    best_opt = ctx->opt;
+                }
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->prof = prof;
+    ctx->opt = rc == RGS_OK ? best_opt : saved;
+    if (rc == RGS_OK && chosen) *chosen = ctx->opt;
+    return rc;
 }
 
 int rgs_trainer_get_grads(rgs_ctx* ctx, float* out) {

@@ -256,33 +256,37 @@ __global__ void __launch_bounds__(128) k_geom_gauss(const float4* __restrict__ p
     const float4* params = MODE == 1 ? a.params : params_in;
     const float4 p0 = params[i];
     const float pos[3] = {p0.x, p0.y, p0.z};
-    // ---- SH planes: sum_v mask_v[ch] * basis_v, then Adam / store per plane
-#pragma unroll 1
-    for (int kq = 0; kq < 4; ++kq) {
-        float4 gr = make_float4(0.0f, 0.0f, 0.0f, 0.0f), gg = gr, gb = gr;
-        for (int v = 0; v < nviews; ++v) {
-            const size_t s = (size_t)v * n + i;
-            if (cnt[s] == 0) continue;
-            const float4 m2 = gv[2 * S + s], m3 = gv[3 * S + s];
-            const float mr = m2.w, mg = m3.x, mb = m3.y;
-            if (mr == 0.0f && mg == 0.0f && mb == 0.0f) continue;
-            float d[3], basis[16];
-            view_dir(pos, cams[v].pos, d);
-            sh_basis(d, basis);
-            const float b0 = basis[kq * 4 + 0], b1 = basis[kq * 4 + 1], b2 = basis[kq * 4 + 2], b3 = basis[kq * 4 + 3];
-            gr.x += mr * b0; gr.y += mr * b1; gr.z += mr * b2; gr.w += mr * b3;
-            gg.x += mg * b0; gg.y += mg * b1; gg.z += mg * b2; gg.w += mg * b3;
-            gb.x += mb * b0; gb.y += mb * b1; gb.z += mb * b2; gb.w += mb * b3;
-        }
-        const float4 gch[3] = {gr, gg, gb};
+    // ---- SH planes: sum_v mask_v[ch] * basis_v (the basis once per view, all
+    // 48 sums in registers), then Adam / store per plane
+    float shg[3][16];
 #pragma unroll
-        for (int ch = 0; ch < 3; ++ch) {
+    for (int ch = 0; ch < 3; ++ch)
+#pragma unroll
+        for (int k = 0; k < 16; ++k) shg[ch][k] = 0.0f;
+    for (int v = 0; v < nviews; ++v) {
+        const size_t s = (size_t)v * n + i;
+        if (cnt[s] == 0) continue;
+        const float4 m2 = gv[2 * S + s], m3 = gv[3 * S + s];
+        const float mk[3] = {m2.w, m3.x, m3.y};
+        if (mk[0] == 0.0f && mk[1] == 0.0f && mk[2] == 0.0f) continue;
+        float d[3], basis[16];
+        view_dir(pos, cams[v].pos, d);
+        sh_basis(d, basis);
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch)
+#pragma unroll
+            for (int k = 0; k < 16; ++k) shg[ch][k] += mk[ch] * basis[k];
+    }
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+#pragma unroll
+        for (int kq = 0; kq < 4; ++kq) {
             const int p = 3 + ch * 4 + kq;
             const size_t o = (size_t)p * cap + i;
+            float4 g = make_float4(shg[ch][kq * 4 + 0], shg[ch][kq * 4 + 1], shg[ch][kq * 4 + 2], shg[ch][kq * 4 + 3]);
             if (MODE == 1) {
-                a.params[o] = adam_plane(p, i, cap, a.params[o], gch[ch], a, bc1, bc2);
+                a.params[o] = adam_plane(p, i, cap, a.params[o], g, a, bc1, bc2);
             } else {
-                float4 g = gch[ch];
                 if (accumulate) {
                     const float4 old = grads[o];
                     g.x += old.x; g.y += old.y; g.z += old.z; g.w += old.w;

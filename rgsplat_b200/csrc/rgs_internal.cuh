@@ -163,9 +163,11 @@ struct BlendArgs {
     int rect_filter;               // per-pixel reference-tile membership test
     int empty_tile_black;          // pixels of empty reference tiles render 0, not bg
     int pixels_per_thread;         // 1 or 2 vertically adjacent pixels per thread
+    float* tstore;                 // store-all variant only: T per (list position, tile pixel)
 };
 void launch_blend_forward(const BlendArgs& a, int tile_w, int tile_h, int batch, cudaStream_t st);
 void launch_blend_backward(const BlendArgs& a, int tile_w, int tile_h, int batch, cudaStream_t st);
+void launch_blend_store_all(const BlendArgs& a, bool fwd, cudaStream_t st);
 
 // loss.cu
 void launch_loss(const DevCam* cams, int nviews, int total_blocks, const float* rgb, float lambda,

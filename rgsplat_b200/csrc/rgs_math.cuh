@@ -119,6 +119,37 @@ __device__ __forceinline__ float expf_fast(float x) {
     return p * __int_as_float((ki + 127) << 23);
 }
 
+// expf_fast restricted to x in [-87, 0] (or NaN), where none of its special
+// cases (overflow, underflow, subnormal scaling) can occur: the same
+// operations in the same order, so the result is bit-identical to
+// expf_fast(x) on that domain. The blend kernels call it only for
+// power in [ln(1 / (255 opacity)) - 0.01, 0], a subset of it.
+__device__ __forceinline__ float expf_fast_nonpos(float x) {
+    const float L2E = 1.44269502f;
+    const float SHIFT = 12582912.0f;
+    const float LN2_HI = 0.693145751953125f;
+    const float LN2_LO = 1.42860677e-06f;
+    float j = __fmaf_rn(x, L2E, SHIFT);
+    float k = j - SHIFT;
+    float rh = __fmaf_rn(-k, LN2_HI, x);
+    float rl = -k * LN2_LO;
+    float q = 2.48015873e-05f;
+    q = __fmaf_rn(q, rh, 1.98412698e-4f);
+    q = __fmaf_rn(q, rh, 1.38888889e-3f);
+    q = __fmaf_rn(q, rh, 8.33333333e-3f);
+    q = __fmaf_rn(q, rh, 4.16666667e-2f);
+    q = __fmaf_rn(q, rh, 1.66666667e-1f);
+    q = __fmaf_rn(q, rh, 0.5f);
+    float hi = 1.0f + rh;
+    float lo = (1.0f - hi) + rh;
+    float s = rh * rh;
+    float tail = __fmaf_rn(s, q, lo);
+    float ea = hi + tail;
+    tail = __fmaf_rn(rl, ea, tail);
+    float p = hi + tail;
+    return p * __int_as_float(((int)k + 127) << 23);
+}
+
 // Rust f32::max / f32::min ignore a NaN operand (fmaxf/fminf do the same);
 // f32::clamp propagates NaN.
 __device__ __forceinline__ float rclamp(float x, float lo, float hi) {

@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(SORT_THREADS) k_upsweep(const uint32_t* __rest
         uint32_t s = 0;
 #pragma unroll
         for (int k = 0; k < SORT_WARPS; ++k) s += s_h[k][d];
-        hist[(size_t)blockIdx.x * R + d] = s;
+        hist[(size_t)d * gridDim.x + blockIdx.x] = s;  // digit-major: hist[d][b]
     }
 }
 
@@ -90,31 +90,48 @@ __device__ __forceinline__ void block_exclusive_scan(uint32_t (&v)[D], uint32_t*
     __syncthreads();
 }
 
+// Turns the digit-major histogram hist[d][b] into global scatter offsets.
+// Digit-major order is exactly the order of the output (all of digit 0 over
+// blocks 0..G-1, then digit 1, ...), so this is one exclusive scan of the
+// R * G counts: every thread sums a contiguous run, the CTA scans the run
+// totals, and every thread rewrites its run as running offsets.
+constexpr int SCAN_THREADS = 1024;
 template <int BITS>
-__global__ void __launch_bounds__(SORT_THREADS) k_scan_hist(uint32_t* __restrict__ hist, int G) {
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_hist(uint32_t* __restrict__ hist, int G) {
     constexpr int R = 1 << BITS;
-    constexpr int D = R / SORT_THREADS;
-    __shared__ uint32_t s_warp[SORT_WARPS];
-    int tid = threadIdx.x;
-    uint32_t tot[D];
+    constexpr int NW = SCAN_THREADS / 32;
+    __shared__ uint32_t s_w[NW];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int n = R * G;
+    const int per = (n + SCAN_THREADS - 1) / SCAN_THREADS;
+    const int b0 = min(tid * per, n), b1 = min(b0 + per, n);
+    uint32_t sum = 0;
+#pragma unroll 8
+    for (int b = b0; b < b1; ++b) sum += hist[b];
+    uint32_t x = sum;
 #pragma unroll
-    for (int k = 0; k < D; ++k) {
-        int d = tid * D + k;
-        uint32_t s = 0;
-        for (int b = 0; b < G; ++b) s += hist[(size_t)b * R + d];
-        tot[k] = s;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
     }
-    uint32_t total;
-    block_exclusive_scan<D>(tot, s_warp, total);
+    if (lane == 31) s_w[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        uint32_t t = s_w[lane];
 #pragma unroll
-    for (int k = 0; k < D; ++k) {
-        int d = tid * D + k;
-        uint32_t run = tot[k];
-        for (int b = 0; b < G; ++b) {
-            uint32_t c = hist[(size_t)b * R + d];
-            hist[(size_t)b * R + d] = run;
-            run += c;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
         }
+        s_w[lane] = t;
+    }
+    __syncthreads();
+    uint32_t run = (w > 0 ? s_w[w - 1] : 0u) + x - sum;
+#pragma unroll 8
+    for (int b = b0; b < b1; ++b) {
+        const uint32_t c = hist[b];
+        hist[b] = run;
+        run += c;
     }
 }
 
@@ -135,7 +152,7 @@ __global__ void __launch_bounds__(SORT_THREADS) k_downsweep(const uint32_t* __re
     int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     uint32_t n = load_n(n_dev, n_host), begin, end;
     chunk_of(n, gridDim.x, blockIdx.x, begin, end);
-    for (int d = tid; d < R; d += SORT_THREADS) s_run[d] = hist[(size_t)blockIdx.x * R + d];
+    for (int d = tid; d < R; d += SORT_THREADS) s_run[d] = hist[(size_t)d * gridDim.x + blockIdx.x];
     const uint32_t lt_mask = (1u << lane) - 1u;
     for (uint32_t base = begin; base < end; base += SORT_TILE) {
         for (int i = tid; i < SORT_WARPS * R; i += SORT_THREADS) (&s_wcnt[0][0])[i] = 0;
@@ -209,7 +226,7 @@ int sort_grid_blocks() {
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        g = sms * 2;
+        g = sms * 4;
     }
     return g;
 }
@@ -231,7 +248,7 @@ int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n_host, const uint
     while (shift < bits) {
         uint32_t* hist = sc.hist.as<uint32_t>();
         k_upsweep<8><<<grid, SORT_THREADS, 0, st>>>(k[cur], n_dev, n_host, shift, hist);
-        k_scan_hist<8><<<1, SORT_THREADS, 0, st>>>(hist, grid);
+        k_scan_hist<8><<<1, SCAN_THREADS, 0, st>>>(hist, grid);
         k_downsweep<8><<<grid, SORT_THREADS, 0, st>>>(k[cur], v[cur], k[cur ^ 1], v[cur ^ 1], n_dev, n_host, shift, hist);
         cur ^= 1;
         shift += 8;

@@ -33,7 +33,8 @@ def tile_lists(gaussians, camera: Camera, ctx: Context | None = None):
     g = _gauss(gaussians)
     n = g.shape[0]
     cam = camera_c(camera)
-    tw, th = ctx.options.tile_w, ctx.options.tile_h
+    o = ctx.options()
+    tw, th = o["tile_w"], o["tile_h"]
     tiles = ((camera.width + tw - 1) // tw) * ((camera.height + th - 1) // th)
     npairs = C.c_uint64(0)
     ip = C.POINTER(C.c_int32)

@@ -1,0 +1,116 @@
+"""Differentiation check on the 50k-Gaussian, 512x512 workload.
+
+* GPU analytic gradients vs the oracle's float analytic gradients (the
+  reference algorithm, src/cpu/backward.rs:107-149): 1e-3 relative.
+* GPU analytic gradients vs FP64 central finite differences at 256 sampled
+  parameters (tests/golden/fd_config2.npz, made by
+  tests/golden/make_fd_config2.py from the oracle in double precision, with
+  eps 1e-4 and, where a 1e-4 step crosses an alpha cut-off, eps 1e-6).
+* The recompute-from-final-T backward vs the store-all-T variant: same
+  gradients, and the blend state each keeps.
+"""
+import importlib.util
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+import rgsplat_b200 as R
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD_PATH = os.path.join(HERE, "golden", "fd_config2.npz")
+
+# Gaussian3D record index -> GaussianGrad index (backward.rs:33-41)
+REC2GRAD = {0: 0, 1: 1, 2: 2, 3: 10, 4: 3, 5: 4, 6: 5, 7: 6, 8: 7, 9: 8, 10: 9}
+REC2GRAD.update({k: k for k in range(11, 59)})
+
+
+def _maker():
+    spec = importlib.util.spec_from_file_location("make_fd_config2", os.path.join(HERE, "golden", "make_fd_config2.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m
+
+
+@pytest.fixture(scope="module")
+def workload():
+    m = _maker()
+    g, cam, target = m.workload()
+    gold = np.load(GOLD_PATH)
+    assert m.digest(g, target) == str(gold["scene_sha256"]), "scene generator drifted from the golden fixture"
+    return g, cam, target, gold
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    return R.Context()
+
+
+def fd_agrees(a, n, scale):
+    """Analytic (float) vs an FP64 central difference: 2 % relative, or an
+    absolute floor of 1e-3 of the largest sampled derivative."""
+    return abs(a - n) <= 0.02 * max(abs(a), abs(n)) + 1e-3 * scale
+
+
+def test_config2_gradients_match_oracle_and_finite_differences(workload, ctx):
+    g, cam, target, gold = workload
+    loss, grads, rep = R.render_and_backward_variant(g, cam, target, store_all=False, ctx=ctx)
+    ref = O.render_and_backward(g, cam, target)
+    assert abs(loss - ref.loss) <= 1e-4 * ref.loss
+    assert abs(loss - float(gold["loss_fp64"])) <= 1e-4 * float(gold["loss_fp64"])
+    e = np.linalg.norm(grads - ref.grads) / np.linalg.norm(ref.grads)
+    assert e < 1e-3, f"relative gradient error vs oracle {e:.2e}"
+
+    gauss, field = gold["gauss"], gold["field"]
+    fds = (gold["fd"], gold["fd_fine"])  # eps 1e-4 and 1e-6
+    scale = np.abs(gold["fd"]).max()
+    rot = (field >= 4) & (field <= 7)
+    bad, coarse_only = [], 0
+    for k in np.nonzero(~rot)[0]:
+        i, f = int(gauss[k]), int(field[k])
+        a = float(grads[i, REC2GRAD[f]])
+        ok = [fd_agrees(a, d[k], scale) for d in fds]
+        coarse_only += not ok[0]
+        if not any(ok):
+            bad.append((i, f, a, fds[0][k], fds[1][k]))
+    # rotation: the last 8 Gaussians carry all four components; the loss sees
+    # only q / |q|, so compare the tangent parts
+    groups = {}
+    for k in np.nonzero(rot)[0]:
+        groups.setdefault(int(gauss[k]), []).append(k)
+    for i, ks in groups.items():
+        assert len(ks) == 4
+        q = g[i, 4:8].astype(np.float64)
+        q /= np.linalg.norm(q)
+        a = grads[i, 3:7].astype(np.float64)
+        pa = a - np.dot(a, q) * q
+        ok = []
+        for d in fds:
+            n = np.array([d[k] for k in ks])
+            pn = n - np.dot(n, q) * q
+            ok.append(np.linalg.norm(pa - pn) <= 0.02 * max(np.linalg.norm(pa), np.linalg.norm(pn)) + 1e-3 * scale)
+        coarse_only += 4 * (not ok[0])
+        if not any(ok):
+            bad.append((i, "rotation", pa))
+    assert int((~rot).sum()) + 4 * len(groups) == 256
+    # every sample matches a central difference; a 1e-4 step that jumps an
+    # alpha cut-off is resolved by the 1e-6 one (positions mostly)
+    assert not bad, f"{len(bad)} of 256 disagree with both differences: {bad[:8]}"
+    assert coarse_only <= 0.1 * 256
+
+
+def test_store_all_backward_matches_recompute(workload, ctx):
+    g, cam, target, _ = workload
+    l0, g0, r0 = R.render_and_backward_variant(g, cam, target, store_all=False, ctx=ctx)
+    l1, g1, r1 = R.render_and_backward_variant(g, cam, target, store_all=True, ctx=ctx)
+    assert l0 == l1
+    e = np.linalg.norm(g1 - g0) / np.linalg.norm(g0)
+    assert e < 1e-5, f"store-all vs recompute {e:.2e}"
+    assert r0["pairs"] == r1["pairs"] > 0
+    px = cam.width * cam.height
+    assert r0["state_bytes"] == px * 8
+    assert r1["state_bytes"] == px * 8 + r1["pairs"] * 256 * 4
+    assert r0["backward_ms"] > 0 and r1["backward_ms"] > 0

@@ -127,6 +127,56 @@ def test_tile_shapes_keep_reference_semantics(tile, ppt, batch):
     assert e < 1e-3
 
 
+def test_autotune_keeps_results_and_state():
+    g, cams, targets = multi_view_scene(n=3000, seed=31)
+    ta = R.Trainer(g, cams, targets)
+    tb = R.Trainer(g, cams, targets)
+    ta.step([0, 1], mode=R.Trainer.BATCHED)
+    tb.step([0, 1], mode=R.Trainer.BATCHED)
+    before = tb.gaussians()
+    st_before = tb.adam_state()
+    pick, table = tb.autotune([2, 3, 4], reps=1)
+    assert len(table) == 18 and all(e["ms"] > 0 for e in table)
+    assert {(e["tile"], e["batch"], e["pixels_per_thread"]) for e in table} == {
+        (t, b, p) for t in ("16x16", "8x32", "32x8") for b in (128, 256, 512) for p in (1, 2)}
+    best = min(table, key=lambda e: e["ms"])
+    assert pick == {k: best[k] for k in ("tile", "batch", "pixels_per_thread")}
+    o = tb.ctx.options()
+    assert f"{o['tile_w']}x{o['tile_h']}" == pick["tile"] and o["batch"] == pick["batch"]
+    # the tuner touches neither parameters nor the Adam state
+    assert np.array_equal(tb.gaussians().view(np.uint32), before.view(np.uint32))
+    st_after = tb.adam_state()
+    assert st_after.t == st_before.t and np.array_equal(st_after.m1, st_before.m1)
+    assert np.array_equal(st_after.grad_accum, st_before.grad_accum)
+    # and the tuned layout trains like the default one (gradients differ only
+    # in the order of their float atomic additions, already after the first
+    # step above)
+    steps = ([2, 3], [5, 1, 0])
+    for vs in steps:
+        la = ta.step(vs, mode=R.Trainer.BATCHED)
+        lb = tb.step(vs, mode=R.Trainer.BATCHED)
+        assert np.allclose(la, lb, rtol=1e-4)
+    assert (np.abs(ta.gaussians() - tb.gaussians()) <= (len(steps) + 1) * step_tolerance()[None, :]).all()
+
+
+def test_step_with_host_targets_matches_resident_targets():
+    g, cams, targets = multi_view_scene(n=3000, seed=32)
+    ta = R.Trainer(g, cams, targets)
+    # the second trainer holds no device targets at all: every step brings its own
+    tb = R.Trainer(g, cams)
+    host = [np.ascontiguousarray(t, np.float32) for t in targets]
+    steps = ([0, 1, 2], [3, 4], [5, 0, 3, 1])
+    for i, vs in enumerate(steps):
+        la = ta.step(vs, mode=R.Trainer.BATCHED)
+        lb = tb.step_host_targets(vs, [host[v].ctypes.data for v in vs])
+        if i == 0:
+            assert np.array_equal(la, lb)
+        else:
+            assert np.allclose(la, lb, rtol=1e-4)
+    assert (np.abs(ta.gaussians() - tb.gaussians()) <= len(steps) * step_tolerance()[None, :]).all()
+    assert tb.adam_state().t == len(steps)
+
+
 def test_trainer_densify_matches_oracle():
     g, cams, targets = multi_view_scene(n=2000, seed=26)
     tr = R.Trainer(g, cams, targets)
