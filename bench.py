@@ -291,11 +291,24 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     tcfg = R.TrainConfig()
     lcfg = R.LossConfig(0.2)
     rng_state = [0x9E3779B97F4A7C15 ^ (rank * 0x5851F42D4C957F2D)]
-    schedule = [xorshift_views(rng_state, len(cfg.cameras), V) for _ in range(args.warmup + 3 * args.steps + 8)]
+    schedule = [xorshift_views(rng_state, len(cfg.cameras), V) for _ in range(args.warmup + max(args.steps, 1))]
+    # warm-up steps take the first view sets; every timed run (batched, plain,
+    # end to end) cycles through the same args.steps view sets after them
+    timed_views = schedule[args.warmup:]
     it = iter(schedule)
 
+    def next_views():
+        try:
+            return next(it)
+        except StopIteration:
+            v = timed_views[next_views.k % len(timed_views)]
+            next_views.k += 1
+            return v
+
+    next_views.k = 0
+
     def step_batched():
-        views = next(it)
+        views = next_views()
         if world == 1:
             return trainer.step(views, mode=R.Trainer.BATCHED, loss_cfg=lcfg, train_cfg=tcfg)
         losses = trainer.backward(views, loss_cfg=lcfg, mode=R.Trainer.BATCHED)
@@ -306,7 +319,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         return losses
 
     def step_plain():
-        views = next(it)
+        views = next_views()
         if world == 1:
             return trainer.step(views, mode=R.Trainer.PLAIN, loss_cfg=lcfg, train_cfg=tcfg)
         losses = trainer.backward(views, loss_cfg=lcfg, mode=R.Trainer.PLAIN)
@@ -371,6 +384,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     kp = args.plain_steps if args.plain_steps is not None else max(3, args.steps // 2)
     with torch.cuda.stream(stream):
         step_plain()
+    next_views.k = 0
     t_plain = timed(step_plain, kp)
 
     # e2e: the step's inputs (8 RGBA targets + cameras) copied from pinned host
@@ -388,7 +402,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         h2d = [0]
 
         def step_e2e():
-            views = schedule[-1 - (step_e2e.k % 8)]
+            # the same view sets as the timed batched steps, so the two numbers
+            # cover the same pixels and pairs
+            views = timed_views[step_e2e.k % len(timed_views)]
             step_e2e.k += 1
             ts = [pinned_target(v) for v in views]
             h2d[0] = sum(t.numel() * 4 for t in ts) + len(views) * 100
@@ -406,7 +422,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             return losses
 
         step_e2e.k = 0
-        for v in set(x for vs in schedule[-8:] for x in vs):
+        for v in set(x for vs in timed_views for x in vs):
             pinned_target(v)
         with torch.cuda.stream(stream):
             step_e2e()
@@ -419,7 +435,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     ms_per_step = t_batched / args.steps * 1e3
 
     # roofline of the dominant stage
-    pixels_per_step = int(np.mean([sum(cfg.cameras[v].width * cfg.cameras[v].height for v in vs) for vs in schedule[: args.steps]]))
+    pixels_per_step = int(np.mean([sum(cfg.cameras[v].width * cfg.cameras[v].height for v in vs) for vs in timed_views]))
     peaks = measured_peaks()
     hbm = peaks.get("hbm_gbs")
     peak_src = "measured"

@@ -15,6 +15,7 @@
 // projection as one 8-byte descriptor (first tile id, width | height << 16),
 // the only per-splat gather of these kernels.
 #include "rgs_internal.cuh"
+#include "tiles.cuh"
 
 namespace rgs {
 
@@ -46,13 +47,13 @@ __device__ __forceinline__ void bin_chunk(uint32_t n, int G, int b, uint32_t& be
 
 __device__ __forceinline__ uint32_t tiles_of(uint2 d) { return (d.y & 0xffffu) * (d.y >> 16); }
 
-__global__ void __launch_bounds__(BIN_THREADS) k_count_reduce(const uint32_t* __restrict__ order, const uint2* __restrict__ tdesc,
+__global__ void __launch_bounds__(BIN_THREADS) k_count_reduce(const uint32_t* __restrict__ order, const uint32_t* __restrict__ cnt,
                                                               uint32_t S, uint32_t* __restrict__ block_sums) {
     __shared__ uint32_t s_w[BIN_THREADS / 32];
     uint32_t begin, end;
     bin_chunk(S, gridDim.x, blockIdx.x, begin, end);
     uint32_t s = 0;
-    for (uint32_t r = begin + threadIdx.x; r < end; r += BIN_THREADS) s += tiles_of(tdesc[order[r]]);
+    for (uint32_t r = begin + threadIdx.x; r < end; r += BIN_THREADS) s += cnt[order[r]];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = s;
@@ -90,9 +91,9 @@ __global__ void __launch_bounds__(1024) k_scan_block_sums(uint32_t* __restrict__
     if (threadIdx.x == 0) *total = s_carry;
 }
 
-void launch_count_scan(const uint32_t* order, const uint2* tdesc, uint32_t S, uint32_t* block_sums, uint32_t* total, int grid,
+void launch_count_scan(const uint32_t* order, const uint32_t* cnt, uint32_t S, uint32_t* block_sums, uint32_t* total, int grid,
                        cudaStream_t st) {
-    k_count_reduce<<<grid, BIN_THREADS, 0, st>>>(order, tdesc, S, block_sums);
+    k_count_reduce<<<grid, BIN_THREADS, 0, st>>>(order, cnt, S, block_sums);
     k_scan_block_sums<<<1, 1024, 0, st>>>(block_sums, grid, total);
 }
 
@@ -211,11 +212,133 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit(const uint32_t* __restrict
     }
 }
 
-void launch_emit_pairs(const uint32_t* order, const uint2* tdesc, uint32_t S, const uint32_t* block_sums, uint32_t* pair_keys,
-                       uint32_t* pair_vals, uint32_t cap, int* overflow, const uint32_t* total, uint32_t* eff,
-                       const DevCam* cams, uint32_t n_per_view, int grid, cudaStream_t st) {
-    k_emit<<<grid, BIN_THREADS, 0, st>>>(order, tdesc, S, block_sums, pair_keys, pair_vals, cap, overflow, total, eff, cams,
-                                         n_per_view);
+// Pruned emission: a slot's pairs are the tiles of its rows' kept spans
+// (tiles.cuh), recomputed here from the stored record exactly as the
+// projection counted them. Each slot of a sub-tile goes to a group of EG
+// lanes, one lane per rectangle row (EG rows at a time): the lanes compute
+// their rows' spans, a group scan turns the span lengths into offsets, and
+// every lane writes its row's run of consecutive pairs. The warp's groups
+// step together for the tallest of their rectangles.
+constexpr int EG = 8;
+__global__ void __launch_bounds__(BIN_THREADS) k_emit_pruned(const uint32_t* __restrict__ order, const uint2* __restrict__ tdesc,
+                                                             const uint32_t* __restrict__ cnt, const float4* __restrict__ rec,
+                                                             uint32_t S, const uint32_t* __restrict__ block_sums,
+                                                             uint32_t* __restrict__ pkeys, uint32_t* __restrict__ pvals,
+                                                             uint32_t cap, int* __restrict__ overflow,
+                                                             const uint32_t* __restrict__ total, uint32_t* __restrict__ eff,
+                                                             const DevCam* __restrict__ cams, uint32_t n_per_view, int tile_w,
+                                                             int tile_h) {
+    __shared__ uint32_t s_off[BIN_SUB + 1];
+    __shared__ uint32_t s_slot[BIN_SUB];
+    __shared__ uint32_t s_w[BIN_THREADS / 32];
+    constexpr int PER = BIN_SUB / BIN_THREADS;
+    constexpr int NGROUPS = BIN_THREADS / EG;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int grp = tid / EG, gl = tid % EG;
+    uint32_t begin, end;
+    bin_chunk(S, gridDim.x, blockIdx.x, begin, end);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *eff = min(*total, cap);
+    uint32_t base = block_sums[blockIdx.x];
+    for (uint32_t r0 = begin; r0 < end; r0 += BIN_SUB) {
+        uint32_t c[PER], local = 0;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const uint32_t r = r0 + (uint32_t)(tid * PER + k);
+            const uint32_t slot = r < end ? order[r] : 0u;
+            c[k] = r < end ? cnt[slot] : 0u;
+            s_slot[tid * PER + k] = slot;
+            local += c[k];
+        }
+        uint32_t x = local;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) s_w[w] = x;
+        __syncthreads();
+        uint32_t wpre = 0, sub_total = 0;
+        for (int k = 0; k < BIN_THREADS / 32; ++k) {
+            uint32_t t = s_w[k];
+            if (k < w) wpre += t;
+            sub_total += t;
+        }
+        uint32_t run = wpre + x - local;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            s_off[tid * PER + k] = run;
+            run += c[k];
+        }
+        if (tid == 0) s_off[BIN_SUB] = sub_total;
+        __syncthreads();
+        for (int k0 = 0; k0 < BIN_SUB; k0 += NGROUPS) {
+            const int k = k0 + grp;
+            const uint32_t nk = s_off[k + 1] - s_off[k];
+            const uint32_t out0 = base + s_off[k];
+            uint32_t slot = 0, tbase = 0;
+            int cx0 = 0, cx1 = 0, ty0 = 0, rows = 0, tiles_x = 1, height = 0;
+            SpanSetup u{};
+            if (nk) {
+                slot = s_slot[k];
+                const uint2 d = tdesc[slot];
+                const DevCam* cam = cams + slot / n_per_view;
+                tiles_x = cam->tiles_x;
+                height = cam->height;
+                tbase = (uint32_t)cam->tile_base;
+                const int lt = (int)d.x - cam->tile_base;
+                ty0 = lt / tiles_x;
+                cx0 = lt - ty0 * tiles_x;
+                cx1 = cx0 + (int)(d.y & 0xffffu);
+                rows = (int)(d.y >> 16);
+                const float4 A = rec[slot], Q = rec[S + slot];
+                u = span_setup(A.x, A.y, Q.x, Q.y, Q.z, power_floor(A.z));
+            }
+            const int steps = __reduce_max_sync(0xffffffffu, (rows + EG - 1) / EG);
+            uint32_t written = 0;
+            for (int it = 0; it < steps; ++it) {
+                const int row = it * EG + gl;
+                int c0 = 0, c1 = 0;
+                if (row < rows) kept_cols(u, ty0 + row, tile_w, tile_h, height, cx0, cx1, c0, c1);
+                const uint32_t span = (uint32_t)(c1 - c0);
+                uint32_t incl = span;
+#pragma unroll
+                for (int o = 1; o < EG; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o, EG);
+                    if (gl >= o) incl += y;
+                }
+                const uint32_t gtot = __shfl_sync(0xffffffffu, incl, EG - 1, EG);
+                uint32_t p = written + incl - span;
+                const uint32_t key0 = tbase + (uint32_t)((ty0 + row) * tiles_x + c0);
+                for (uint32_t t = 0; t < span; ++t, ++p) {
+                    const uint32_t out = out0 + p;
+                    if (p < nk && out < cap) {
+                        pkeys[out] = key0 + t;
+                        pvals[out] = slot;
+                    } else {
+                        *overflow = 1;
+                    }
+                }
+                written += gtot;
+            }
+            // the projection counted the same spans; a disagreement would
+            // leave stale pairs, so it fails the step
+            if (gl == 0 && written != nk) *overflow = 1;
+        }
+        base += sub_total;
+        __syncthreads();
+    }
+}
+
+void launch_emit_pairs(const uint32_t* order, const uint2* tdesc, const uint32_t* cnt, const float4* rec, uint32_t S,
+                       const uint32_t* block_sums, uint32_t* pair_keys, uint32_t* pair_vals, uint32_t cap, int* overflow,
+                       const uint32_t* total, uint32_t* eff, const DevCam* cams, uint32_t n_per_view, int tile_w,
+                       int tile_h, int prune, int grid, cudaStream_t st) {
+    if (prune)
+        k_emit_pruned<<<grid, BIN_THREADS, 0, st>>>(order, tdesc, cnt, rec, (uint32_t)S, block_sums, pair_keys, pair_vals, cap,
+                                                    overflow, total, eff, cams, n_per_view, tile_w, tile_h);
+    else
+        k_emit<<<grid, BIN_THREADS, 0, st>>>(order, tdesc, S, block_sums, pair_keys, pair_vals, cap, overflow, total, eff, cams,
+                                             n_per_view);
 }
 
 // Tile boundaries of the sorted pair keys: each thread takes four consecutive

@@ -35,6 +35,7 @@
 
 #include "rgs_internal.cuh"
 #include "rgs_math.cuh"
+#include "tiles.cuh"
 
 namespace rgs {
 
@@ -47,36 +48,6 @@ __device__ __forceinline__ int find_view(const DevCam* cams, int nviews, int til
 __device__ __forceinline__ bool in_rect(float rx, float ry, int px, int py) {
     uint32_t x = __float_as_uint(rx), y = __float_as_uint(ry);
     return px >= (int)(x & 0xffffu) && px < (int)(x >> 16) && py >= (int)(y & 0xffffu) && py < (int)(y >> 16);
-}
-
-// Power below which alpha = min(op * e^power, 0.99) < 1/255 for this opacity
-// (op <= 1 and op >= 1/255 for every projected splat), with a 1 % margin in
-// alpha that covers the rounding of op * exp and of this logarithm.
-__device__ __forceinline__ float power_floor(float op) { return -__logf(255.0f * op) - 0.01f; }
-
-// Conservative tile test: true only if every pixel centre of the box has
-// power = -q/2 < thr, where q = a dx^2 + 2 b dx dy + c dy^2 (the reference's
-// expression, backward.rs:340). The box minimum of the convex q lies on an
-// edge unless the splat centre is inside; each edge is a 1-D quadratic. Only
-// well-conditioned conics (ac - b^2 >= ac / 100, so the float evaluation of q
-// here and per pixel is accurate to ~1e-4 relative) are tested, with a 1e-3
-// margin; anything else (including NaN) is kept.
-__device__ __forceinline__ bool tile_rejects(float sx, float sy, float a, float b, float c, float thr, float x0c, float x1c,
-                                             float y0c, float y1c) {
-    if (!(a > 0.0f && c > 0.0f && (a * c - b * b) >= 0.01f * (a * c))) return false;
-    const float lx = x0c - sx, hx = x1c - sx, ly = y0c - sy, hy = y1c - sy;
-    if (lx <= 0.0f && hx >= 0.0f && ly <= 0.0f && hy >= 0.0f) return false;
-    float best = __int_as_float(0x7f800000);
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-        const float dx = e ? hx : lx;
-        const float dy = fminf(fmaxf(-b * dx / c, ly), hy);
-        best = fminf(best, a * dx * dx + 2.0f * b * dx * dy + c * dy * dy);
-        const float ey = e ? hy : ly;
-        const float ex = fminf(fmaxf(-b * ey / a, lx), hx);
-        best = fminf(best, a * ex * ex + 2.0f * b * ex * ey + c * ey * ey);
-    }
-    return best * 0.999f > -2.0f * thr;
 }
 
 // Stages the tile-list entries [first, end) (at most BATCH) into shared memory,
@@ -104,7 +75,7 @@ __device__ __forceinline__ int stage_batch(const BlendArgs& a, size_t S, uint32_
             Q = a.rec[S + slot];
             K = a.rec[2 * S + slot];
             A.w = power_floor(A.z);
-            keep = !tile_rejects(A.x, A.y, Q.x, Q.y, Q.z, A.w, x0c, x1c, y0c, y1c);
+            keep = !tile_rejects(tile_test_setup(A.x, A.y, Q.x, Q.y, Q.z, A.w), x0c, x1c, y0c, y1c);
             if (s_rall) s_rall[j] = make_uint2(__float_as_uint(Q.w), __float_as_uint(K.w));
         }
         const unsigned m = __ballot_sync(0xffffffffu, keep);

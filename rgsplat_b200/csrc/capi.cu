@@ -377,15 +377,19 @@ struct Binned {
 
 // Projection + depth sort + pair emission + tile sort + ranges for one batch.
 // `k_host` >= 0 means the pair count was read back (plain path).
+// prune: tile lists hold only the (tile, splat) pairs the blend's own tile
+// test keeps (exact: the blend drops the others from every batch anyway).
+// Only valid with a zero background, where a pixel whose reference tile list
+// is empty renders the same 0 as one whose splats all miss it.
 int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tiles, bool host_count, Binned& out,
-              bool project = true) {
+              bool project = true, bool prune = false) {
     cudaStream_t st = ctx->st;
     const size_t S = (size_t)s.n * V;
     uint32_t* sc = ctx->scalars.as<uint32_t>();
     if (project)
         launch_project(s.params.as<float4>(), s.n, s.cap, cams_dev, V, ctx->opt.tile_w, ctx->opt.tile_h,
                        ctx->rec.as<float4>(), ctx->cnt.as<uint32_t>(), ctx->tdesc.as<uint2>(), ctx->dkey.as<uint32_t>(),
-                       ctx->ids.as<uint32_t>(), st);
+                       ctx->ids.as<uint32_t>(), prune ? 1 : 0, st);
     mark(ctx, 1);
     cudaError_t e;
     int which = radix_sort_pairs(ctx->dkey.as<uint32_t>(), ctx->ids.as<uint32_t>(), (uint32_t)S, nullptr, 32, ctx->sort,
@@ -393,7 +397,7 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
     if (e != cudaSuccess) return cuda_fail(ctx, e, "depth sort");
     mark(ctx, 2);
     const uint32_t* order = which ? ctx->sort.vals2.as<uint32_t>() : ctx->ids.as<uint32_t>();
-    launch_count_scan(order, ctx->tdesc.as<uint2>(), (uint32_t)S, ctx->block_sums.as<uint32_t>(), sc + SC_PAIRS,
+    launch_count_scan(order, ctx->cnt.as<uint32_t>(), (uint32_t)S, ctx->block_sums.as<uint32_t>(), sc + SC_PAIRS,
                       bin_grid_blocks(), st);
     if (host_count) {
         uint32_t K = 0;
@@ -422,9 +426,10 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
         }
     }
     CK(cudaMemsetAsync(sc + SC_OVERFLOW, 0, 4, st));
-    launch_emit_pairs(order, ctx->tdesc.as<uint2>(), (uint32_t)S, ctx->block_sums.as<uint32_t>(), ctx->pkeys.as<uint32_t>(),
-                      ctx->pvals.as<uint32_t>(), ctx->pair_cap, (int*)(sc + SC_OVERFLOW), sc + SC_PAIRS, sc + SC_PAIRS_EFF,
-                      cams_dev, (uint32_t)s.n, bin_grid_blocks(), st);
+    launch_emit_pairs(order, ctx->tdesc.as<uint2>(), ctx->cnt.as<uint32_t>(), ctx->rec.as<float4>(), (uint32_t)S,
+                      ctx->block_sums.as<uint32_t>(), ctx->pkeys.as<uint32_t>(), ctx->pvals.as<uint32_t>(), ctx->pair_cap,
+                      (int*)(sc + SC_OVERFLOW), sc + SC_PAIRS, sc + SC_PAIRS_EFF, cams_dev, (uint32_t)s.n, ctx->opt.tile_w,
+                      ctx->opt.tile_h, prune ? 1 : 0, bin_grid_blocks(), st);
     mark(ctx, 3);
     int which2 = radix_sort_pairs(ctx->pkeys.as<uint32_t>(), ctx->pvals.as<uint32_t>(), ctx->pair_cap, sc + SC_PAIRS_EFF,
                                   bits_for(std::max<size_t>(tiles, 2)), ctx->sort, ctx->sort_grid, st, &e);
@@ -464,6 +469,8 @@ BlendArgs blend_args(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, cons
     return a;
 }
 
+bool zero_bg(const float bg[3]) { return bg[0] == 0.0f && bg[1] == 0.0f && bg[2] == 0.0f; }
+
 // Uploads one view's camera header (plain path) and returns its device copy.
 int upload_single_cam(rgs_ctx* ctx, const DevCam& d, DevCam** dev) {
     StepHdr* h = ctx->hdr_h;
@@ -500,7 +507,7 @@ int run_view_plain(rgs_ctx* ctx, Scene& s, const DevCam& dc_in, const float* tar
     if ((rc = upload_single_cam(ctx, dc, &cams_dev))) return rc;
     mark(ctx, 0);
     Binned b;
-    if ((rc = bin_batch(ctx, s, cams_dev, 1, tiles, true, b))) return rc;
+    if ((rc = bin_batch(ctx, s, cams_dev, 1, tiles, true, b, true, zero_bg(bg)))) return rc;
     BlendArgs fa = blend_args(ctx, s, cams_dev, 1, nullptr, tiles, b, bg, true);
     if (study) {
         // blend state: final T + last contributor per pixel, plus (store-all)
@@ -1122,7 +1129,7 @@ int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], fl
     size_t S = (size_t)s.n * V;
     CK(ctx->sort.keys2.ensure(std::max<size_t>(S, ctx->pair_cap) * 4 + 16));
     CK(ctx->sort.vals2.ensure(std::max<size_t>(S, ctx->pair_cap) * 4 + 16));
-    CK(ctx->sort.hist.ensure((size_t)ctx->sort_grid * 512 * 4));
+    CK(ctx->sort.hist.ensure(sort_hist_bytes(ctx->sort_grid)));
     StepHdr* hd = ctx->hdr.as<StepHdr>();
     const DevCam* cams_dev = (const DevCam*)((char*)ctx->hdr.p + offsetof(StepHdr, cams));
     float* losses_dev = (float*)((char*)ctx->outd.p + offsetof(StepOut, losses));
@@ -1131,7 +1138,7 @@ int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], fl
     cudaMemcpyAsync(ctx->hdr.p, ctx->hdr_h, sizeof(StepHdr), cudaMemcpyHostToDevice, st);
     mark(ctx, 0);
     Binned b;
-    int rc = bin_batch(ctx, s, cams_dev, V, tiles_cap, false, b);
+    int rc = bin_batch(ctx, s, cams_dev, V, tiles_cap, false, b, true, zero_bg(bg));
     if (!rc) {
         BlendArgs fa = blend_args(ctx, s, cams_dev, V, &hd->total_tiles, tiles_cap, b, bg, true);
         launch_blend_forward(fa, ctx->opt.tile_w, ctx->opt.tile_h, ctx->opt.batch, st);

@@ -8,6 +8,7 @@
 // (an integer decision) matches the CPU restatement bit for bit.
 #include "rgs_internal.cuh"
 #include "rgs_math.cuh"
+#include "tiles.cuh"
 
 namespace rgs {
 
@@ -119,7 +120,7 @@ __global__ void __launch_bounds__(256) k_project(const float4* __restrict__ para
                                                  const DevCam* __restrict__ cams, int nviews, int tile_w,
                                                  int tile_h, float4* __restrict__ rec, uint32_t* __restrict__ cnt,
                                                  uint2* __restrict__ tdesc, uint32_t* __restrict__ dkey,
-                                                 uint32_t* __restrict__ ids) {
+                                                 uint32_t* __restrict__ ids, int prune) {
     size_t S = (size_t)n * nviews;
     size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S) return;
@@ -145,18 +146,29 @@ __global__ void __launch_bounds__(256) k_project(const float4* __restrict__ para
     rec[s] = make_float4(o.sx, o.sy, o.opacity, o.depth);
     rec[S + s] = make_float4(o.conic[0], o.conic[1], o.conic[2], __uint_as_float((uint32_t)x0 | ((uint32_t)x1 << 16)));
     rec[2 * S + s] = make_float4(o.color[0], o.color[1], o.color[2], __uint_as_float((uint32_t)y0 | ((uint32_t)y1 << 16)));
-    cnt[s] = (uint32_t)((ctx1 - ctx0) * (cty1 - cty0));
+    uint32_t count = (uint32_t)((ctx1 - ctx0) * (cty1 - cty0));
+    if (prune) {
+        // only the tiles of each row's kept span (tiles.cuh)
+        const SpanSetup u = span_setup(o.sx, o.sy, o.conic[0], o.conic[1], o.conic[2], power_floor(o.opacity));
+        count = 0;
+        for (int ty = cty0; ty < cty1; ++ty) {
+            int c0, c1;
+            kept_cols(u, ty, tile_w, tile_h, c.height, ctx0, ctx1, c0, c1);
+            count += (uint32_t)(c1 - c0);
+        }
+    }
+    cnt[s] = count;
     tdesc[s] = make_uint2((uint32_t)(c.tile_base + cty0 * c.tiles_x + ctx0),
                           (uint32_t)(ctx1 - ctx0) | ((uint32_t)(cty1 - cty0) << 16));
     dkey[s] = __float_as_uint(o.depth);
 }
 
 void launch_project(const float4* params, int n, int cap, const DevCam* cams, int nviews, int tile_w, int tile_h,
-                    float4* rec, uint32_t* cnt, uint2* tdesc, uint32_t* dkey, uint32_t* ids, cudaStream_t st) {
+                    float4* rec, uint32_t* cnt, uint2* tdesc, uint32_t* dkey, uint32_t* ids, int prune, cudaStream_t st) {
     size_t S = (size_t)n * nviews;
     if (S == 0) return;
     unsigned blocks = (unsigned)((S + 255) / 256);
-    k_project<<<blocks, 256, 0, st>>>(params, n, cap, cams, nviews, tile_w, tile_h, rec, cnt, tdesc, dkey, ids);
+    k_project<<<blocks, 256, 0, st>>>(params, n, cap, cams, nviews, tile_w, tile_h, rec, cnt, tdesc, dkey, ids, prune);
 }
 
 // ---------------------------------------------------------------------------

@@ -115,10 +115,11 @@ void launch_check_finite(const float4* planes, int n, int cap, int* flag, cudaSt
 
 // project.cu
 // tdesc[s] = (global id of the splat's first CTA tile, width | height << 16 of
-// its CTA-tile rectangle); zero for culled slots.
+// its CTA-tile rectangle), cnt[s] = its number of CTA tiles, or with prune = 1
+// the number inside the rows' kept spans (tiles.cuh); zero for culled slots.
 void launch_project(const float4* params, int n, int cap, const DevCam* cams, int nviews,
                     int tile_w, int tile_h, float4* rec, uint32_t* cnt, uint2* tdesc, uint32_t* dkey,
-                    uint32_t* ids, cudaStream_t st);
+                    uint32_t* ids, int prune, cudaStream_t st);
 void launch_project_wgsl(const float4* params, int n, int cap, const DevCam* cam, int cpu_math,
                          float* splats10, uint32_t* keys, cudaStream_t st);
 void launch_composite_prepare(const float* splats10, int n, const DevCam* cam, int tile_w, int tile_h,
@@ -131,14 +132,18 @@ void launch_composite_prepare(const float* splats10, int n, const DevCam* cam, i
 int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n_host, const uint32_t* n_dev, int bits,
                      SortScratch& sc, int grid, cudaStream_t st, cudaError_t* err);
 int sort_grid_blocks();
+// scratch of one radix pass: a [256][grid] digit histogram plus 256 digit totals
+inline size_t sort_hist_bytes(int grid) { return ((size_t)grid * 256 + 256) * 4; }
 
 // bin.cu
-void launch_count_scan(const uint32_t* order, const uint2* tdesc, uint32_t S, uint32_t* block_sums,
+// Pair counts come from cnt[] (full or pruned); with prune the emission
+// expands only the tiles of each row's kept span, recomputed from the record.
+void launch_count_scan(const uint32_t* order, const uint32_t* cnt, uint32_t S, uint32_t* block_sums,
                        uint32_t* total, int grid, cudaStream_t st);
-void launch_emit_pairs(const uint32_t* order, const uint2* tdesc, uint32_t S, const uint32_t* block_sums,
-                       uint32_t* pair_keys, uint32_t* pair_vals, uint32_t cap, int* overflow,
-                       const uint32_t* total, uint32_t* eff, const DevCam* cams, uint32_t n_per_view,
-                       int grid, cudaStream_t st);
+void launch_emit_pairs(const uint32_t* order, const uint2* tdesc, const uint32_t* cnt, const float4* rec, uint32_t S,
+                       const uint32_t* block_sums, uint32_t* pair_keys, uint32_t* pair_vals, uint32_t cap, int* overflow,
+                       const uint32_t* total, uint32_t* eff, const DevCam* cams, uint32_t n_per_view, int tile_w,
+                       int tile_h, int prune, int grid, cudaStream_t st);
 int bin_grid_blocks();
 void launch_tile_ranges(const uint32_t* pair_keys, const uint32_t* total, uint32_t cap, uint2* ranges,
                         cudaStream_t st);

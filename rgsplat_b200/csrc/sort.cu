@@ -90,56 +90,49 @@ __device__ __forceinline__ void block_exclusive_scan(uint32_t (&v)[D], uint32_t*
     __syncthreads();
 }
 
-// Turns the digit-major histogram hist[d][b] into global scatter offsets.
-// Digit-major order is exactly the order of the output (all of digit 0 over
-// blocks 0..G-1, then digit 1, ...), so this is one exclusive scan of the
-// R * G counts: every thread sums a contiguous run, the CTA scans the run
-// totals, and every thread rewrites its run as running offsets.
-constexpr int SCAN_THREADS = 1024;
+// Turns the digit-major histogram hist[d][b] into per-digit block offsets
+// (exclusive over blocks b) and writes each digit's total to dtot[d]. One
+// warp per digit: each lane loads its SCAN_PER consecutive-by-32 counts at
+// once (no serial load latency), then the warp scans them chunk by chunk.
+// The digit bases (an exclusive scan of the R totals) are formed by every
+// downsweep CTA itself.
+constexpr int SCAN_WARPS = 8;
+constexpr int SCAN_PER = 32;  // G <= 32 * 32 blocks
 template <int BITS>
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_hist(uint32_t* __restrict__ hist, int G) {
+__global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan_hist(uint32_t* __restrict__ hist, uint32_t* __restrict__ dtot, int G) {
     constexpr int R = 1 << BITS;
-    constexpr int NW = SCAN_THREADS / 32;
-    __shared__ uint32_t s_w[NW];
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int n = R * G;
-    const int per = (n + SCAN_THREADS - 1) / SCAN_THREADS;
-    const int b0 = min(tid * per, n), b1 = min(b0 + per, n);
-    uint32_t sum = 0;
-#pragma unroll 8
-    for (int b = b0; b < b1; ++b) sum += hist[b];
-    uint32_t x = sum;
+    const int lane = threadIdx.x & 31;
+    const int d = blockIdx.x * SCAN_WARPS + (threadIdx.x >> 5);
+    if (d >= R) return;
+    uint32_t* row = hist + (size_t)d * G;
+    uint32_t v[SCAN_PER];
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
+    for (int k = 0; k < SCAN_PER; ++k) {
+        const int b = k * 32 + lane;
+        v[k] = b < G ? row[b] : 0u;
     }
-    if (lane == 31) s_w[w] = x;
-    __syncthreads();
-    if (w == 0) {
-        uint32_t t = s_w[lane];
+    uint32_t carry = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_PER; ++k) {
+        if (k * 32 >= G) break;
+        uint32_t x = v[k];
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
-            if (lane >= o) t += y;
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
         }
-        s_w[lane] = t;
+        const int b = k * 32 + lane;
+        if (b < G) row[b] = carry + x - v[k];
+        carry += __shfl_sync(0xffffffffu, x, 31);
     }
-    __syncthreads();
-    uint32_t run = (w > 0 ? s_w[w - 1] : 0u) + x - sum;
-#pragma unroll 8
-    for (int b = b0; b < b1; ++b) {
-        const uint32_t c = hist[b];
-        hist[b] = run;
-        run += c;
-    }
+    if (lane == 0) dtot[d] = carry;
 }
 
 template <int BITS>
 __global__ void __launch_bounds__(SORT_THREADS) k_downsweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                             uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                             const uint32_t* n_dev, uint32_t n_host, int shift,
-                                                            const uint32_t* __restrict__ hist) {
+                                                            const uint32_t* __restrict__ hist, const uint32_t* __restrict__ dtot) {
     constexpr int R = 1 << BITS;
     constexpr int D = R / SORT_THREADS;
     __shared__ uint32_t s_run[R];
@@ -152,7 +145,17 @@ __global__ void __launch_bounds__(SORT_THREADS) k_downsweep(const uint32_t* __re
     int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     uint32_t n = load_n(n_dev, n_host), begin, end;
     chunk_of(n, gridDim.x, blockIdx.x, begin, end);
-    for (int d = tid; d < R; d += SORT_THREADS) s_run[d] = hist[(size_t)d * gridDim.x + blockIdx.x];
+    {
+        // digit bases: exclusive scan of the digit totals, then this block's
+        // offset within each digit
+        uint32_t tb[D];
+#pragma unroll
+        for (int q = 0; q < D; ++q) tb[q] = dtot[tid * D + q];
+        uint32_t all;
+        block_exclusive_scan<D>(tb, s_warp, all);
+#pragma unroll
+        for (int q = 0; q < D; ++q) s_run[tid * D + q] = tb[q] + hist[(size_t)(tid * D + q) * gridDim.x + blockIdx.x];
+    }
     const uint32_t lt_mask = (1u << lane) - 1u;
     for (uint32_t base = begin; base < end; base += SORT_TILE) {
         for (int i = tid; i < SORT_WARPS * R; i += SORT_THREADS) (&s_wcnt[0][0])[i] = 0;
@@ -238,7 +241,11 @@ int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n_host, const uint
     size_t cap = n_host;
     if ((*err = sc.keys2.ensure(cap * 4 + 16)) != cudaSuccess) return 0;
     if ((*err = sc.vals2.ensure(cap * 4 + 16)) != cudaSuccess) return 0;
-    if ((*err = sc.hist.ensure((size_t)grid * 512 * 4)) != cudaSuccess) return 0;
+    if ((*err = sc.hist.ensure(sort_hist_bytes(grid))) != cudaSuccess) return 0;
+    if (grid > 32 * SCAN_PER) {
+        *err = cudaErrorInvalidValue;
+        return 0;
+    }
     uint32_t* k[2] = {keys, sc.keys2.as<uint32_t>()};
     uint32_t* v[2] = {vals, sc.vals2.as<uint32_t>()};
     int cur = 0;
@@ -247,9 +254,10 @@ int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n_host, const uint
     // (the bits above `bits` are zero in every key, so they do not reorder).
     while (shift < bits) {
         uint32_t* hist = sc.hist.as<uint32_t>();
+        uint32_t* dtot = hist + (size_t)grid * 256;
         k_upsweep<8><<<grid, SORT_THREADS, 0, st>>>(k[cur], n_dev, n_host, shift, hist);
-        k_scan_hist<8><<<1, SCAN_THREADS, 0, st>>>(hist, grid);
-        k_downsweep<8><<<grid, SORT_THREADS, 0, st>>>(k[cur], v[cur], k[cur ^ 1], v[cur ^ 1], n_dev, n_host, shift, hist);
+        k_scan_hist<8><<<256 / SCAN_WARPS, SCAN_WARPS * 32, 0, st>>>(hist, dtot, grid);
+        k_downsweep<8><<<grid, SORT_THREADS, 0, st>>>(k[cur], v[cur], k[cur ^ 1], v[cur ^ 1], n_dev, n_host, shift, hist, dtot);
         cur ^= 1;
         shift += 8;
     }

@@ -95,6 +95,18 @@ def test_forward_matches_oracle(ctx, bg):
     assert np.array_equal(ft.view(np.uint32), oft.view(np.uint32))
 
 
+def test_pruned_tile_lists_render_identically(ctx):
+    # with a zero background the render / training paths bin only the
+    # (tile, splat) pairs the blend's tile test keeps; the image must not change
+    g, cam, _ = small_scene(seed=11)
+    rgb = R.render_color(g, cam, (0.0, 0.0, 0.0), ctx=ctx)
+    pruned = ctx.stats()["pairs"]
+    orgb, _, _ = O.render_color(g, cam, (0.0, 0.0, 0.0))
+    assert np.array_equal(rgb.reshape(-1).view(np.uint32), orgb.reshape(-1).view(np.uint32))
+    _, ent = D.tile_lists(g, cam, ctx)  # the reference's full lists
+    assert 0 < pruned < ent.size
+
+
 def test_render_color_odd_sizes(ctx):
     g, cam, _ = small_scene(n=3000, seed=6, w=173, h=91, fx=200.0)
     rgb = R.render_color(g, cam, (0.1, 0.1, 0.1), ctx=ctx)
