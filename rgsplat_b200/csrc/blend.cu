@@ -55,10 +55,10 @@ __device__ __forceinline__ bool in_rect(float rx, float ry, int px, int py) {
 // li0 is the tile-list index of `first`. Must be called by the whole block.
 // When s_rall is given, every staged entry's pixel rectangle (kept or not) is
 // recorded at its batch position.
-template <int NT, int BATCH>
+template <int NT, int BATCH, int RW, bool WMASK>
 __device__ __forceinline__ int stage_batch(const BlendArgs& a, size_t S, uint32_t first, uint32_t end, int li0, float x0c,
-                                           float x1c, float y0c, float y1c, float4* s_a, float4* s_c, float4* s_k, int* s_li,
-                                           uint32_t* s_slot, int* s_wsum, uint2* s_rall) {
+                                           float x1c, float y0c, float y1c, int ytile, int height, float4* s_a, float4* s_c,
+                                           float4* s_k, int* s_li, uint8_t* s_wm, uint32_t* s_slot, int* s_wsum, uint2* s_rall) {
     constexpr int NW = NT / 32;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     int kept = 0;
@@ -68,14 +68,25 @@ __device__ __forceinline__ int stage_batch(const BlendArgs& a, size_t S, uint32_
         const uint32_t idx = first + (uint32_t)j;
         bool keep = false;
         float4 A, Q, K;
-        uint32_t slot = 0;
+        uint32_t slot = 0, wm = 0;
         if (j < BATCH && idx < end) {
             slot = a.pair_vals[idx];
             A = a.rec[slot];
             Q = a.rec[S + slot];
             K = a.rec[2 * S + slot];
             A.w = power_floor(A.z);
-            keep = !tile_rejects(tile_test_setup(A.x, A.y, Q.x, Q.y, Q.z, A.w), x0c, x1c, y0c, y1c);
+            const TileTest t = tile_test_setup(A.x, A.y, Q.x, Q.y, Q.z, A.w);
+            keep = !tile_rejects(t, x0c, x1c, y0c, y1c);
+            if (WMASK && keep) {
+                // the same test per warp: warp ww owns pixel rows [ww*RW, ww*RW + RW)
+                // of the tile, all its columns
+#pragma unroll
+                for (int ww = 0; ww < NW; ++ww) {
+                    const int r0 = ytile + ww * RW;
+                    const int r1 = min(r0 + RW, height) - 1;
+                    if (r0 <= r1 && !tile_rejects(t, x0c, x1c, (float)r0 + 0.5f, (float)r1 + 0.5f)) wm |= 1u << ww;
+                }
+            }
             if (s_rall) s_rall[j] = make_uint2(__float_as_uint(Q.w), __float_as_uint(K.w));
         }
         const unsigned m = __ballot_sync(0xffffffffu, keep);
@@ -94,6 +105,7 @@ __device__ __forceinline__ int stage_batch(const BlendArgs& a, size_t S, uint32_
             s_c[p] = Q;
             s_k[p] = K;
             s_li[p] = li0 + j;
+            if (WMASK) s_wm[p] = (uint8_t)wm;
             if (s_slot) s_slot[p] = slot;
         }
         kept += total;
@@ -115,6 +127,7 @@ __global__ void __launch_bounds__(TW * TH / PPT) k_blend_fwd(BlendArgs a) {
     __shared__ int s_wsum[NT / 32];
     __shared__ uint2 s_rall[RECT ? BATCH : 1];
     __shared__ int s_tile;
+    constexpr int RW = (32 / TW) * PPT;  // pixel rows per warp
     const int tid = threadIdx.x;
     const int total_tiles = a.total_tiles ? (int)*a.total_tiles : a.total_tiles_host;
     const size_t S = (size_t)a.n_per_view * a.nviews;
@@ -151,8 +164,9 @@ __global__ void __launch_bounds__(TW * TH / PPT) k_blend_fwd(BlendArgs a) {
         for (uint32_t b0 = rg.x; b0 < rg.y; b0 += BATCH) {
             if (__syncthreads_count(!all_done) == 0) break;
             const bool need_seen = RECT && a.empty_tile_black;
-            const int nb = stage_batch<NT, BATCH>(a, S, b0, rg.y, (int)(b0 - rg.x), x0c, x1c, y0c, y1c, s_a, s_c, s_k, s_li,
-                                                  nullptr, s_wsum, need_seen ? s_rall : nullptr);
+            const int nb = stage_batch<NT, BATCH, RW, false>(a, S, b0, rg.y, (int)(b0 - rg.x), x0c, x1c, y0c, y1c, ty * TH,
+                                                             c.height, s_a, s_c, s_k, s_li, nullptr, nullptr, s_wsum,
+                                                             need_seen ? s_rall : nullptr);
             if (need_seen) {
                 // a pixel's reference tile list is non-empty iff some entry (kept
                 // or rejected) covers the pixel
@@ -252,8 +266,12 @@ __device__ __forceinline__ void red_add_v4(float4* addr, float x, float y, float
 
 // Backward. A thread owns PPT vertical pixels; their gradient contributions to
 // a splat are summed in registers before the warp reduction. T is rebuilt as
-// T * 1/(1 - alpha) (one correctly rounded reciprocal serves both uses; the
-// reference divides, backward.rs:452, which differs by an ulp).
+// T * 1/(1 - alpha) with the hardware reciprocal (within 2 ulp; one reciprocal
+// serves both uses, where the reference divides, backward.rs:452): over the
+// at most few hundred splats a pixel rebuilds through, T stays within ~1e-5
+// relative of the reference's, far inside the gradients' 1e-3 tolerance.
+// Alpha itself is recomputed bit for bit as the forward did, so the set of
+// contributing splats is the forward's.
 template <int TW, int TH, int BATCH, bool RECT, int PPT, bool STORE = false>
 __global__ void __launch_bounds__(TW * TH / PPT) k_blend_bwd(BlendArgs a) {
     constexpr int NT = TW * TH / PPT;
@@ -262,12 +280,15 @@ __global__ void __launch_bounds__(TW * TH / PPT) k_blend_bwd(BlendArgs a) {
     __shared__ float4 s_c[BATCH];
     __shared__ float4 s_k[BATCH];
     __shared__ int s_li[BATCH];
+    __shared__ uint8_t s_wm[BATCH];
     __shared__ uint32_t s_slot[BATCH];
     __shared__ float s_acc[BATCH][NACC];
     __shared__ int s_wsum[NT / 32];
     __shared__ int s_tile;
     __shared__ int s_maxlc;
+    constexpr int RW = (32 / TW) * PPT;  // pixel rows per warp
     const int tid = threadIdx.x, lane = tid & 31;
+    const uint32_t wbit = 1u << (tid >> 5);
     const int total_tiles = a.total_tiles ? (int)*a.total_tiles : a.total_tiles_host;
     const size_t S = (size_t)a.n_per_view * a.nviews;
     for (;;) {
@@ -316,8 +337,8 @@ __global__ void __launch_bounds__(TW * TH / PPT) k_blend_bwd(BlendArgs a) {
         const int maxlc = s_maxlc;
         for (int hi = maxlc; hi >= 0; hi -= BATCH) {
             const int lo = max(hi - BATCH + 1, 0);
-            const int nb = stage_batch<NT, BATCH>(a, S, rg.x + (uint32_t)lo, rg.x + (uint32_t)hi + 1u, lo, x0c, x1c, y0c, y1c,
-                                                  s_a, s_c, s_k, s_li, s_slot, s_wsum, nullptr);
+            const int nb = stage_batch<NT, BATCH, RW, true>(a, S, rg.x + (uint32_t)lo, rg.x + (uint32_t)hi + 1u, lo, x0c, x1c, y0c,
+                                                      y1c, ty * TH, c.height, s_a, s_c, s_k, s_li, s_wm, s_slot, s_wsum, nullptr);
             for (int k = tid; k < nb; k += NT) {
 #pragma unroll
                 for (int q = 0; q < NACC; ++q) s_acc[k][q] = 0.0f;
@@ -325,7 +346,7 @@ __global__ void __launch_bounds__(TW * TH / PPT) k_blend_bwd(BlendArgs a) {
             __syncthreads();
             for (int k = nb - 1; k >= 0; --k) {
                 const int li = s_li[k];
-                if (li > warp_maxlc) continue;  // warp-uniform
+                if (li > warp_maxlc || !(s_wm[k] & wbit)) continue;  // warp-uniform
                 float g[NACC];
 #pragma unroll
                 for (int q = 0; q < NACC; ++q) g[q] = 0.0f;
@@ -357,7 +378,7 @@ __global__ void __launch_bounds__(TW * TH / PPT) k_blend_bwd(BlendArgs a) {
                             T[p] = a.tstore[(size_t)(rg.x + (uint32_t)li) * (TW * TH) + (tid / TW) * PPT * TW + p * TW + tid % TW];
                             inv_1ma = 1.0f / (1.0f - alpha);
                         } else {
-                            inv_1ma = __frcp_rn(1.0f - alpha);
+                            inv_1ma = __fdividef(1.0f, 1.0f - alpha);
                             T[p] = T[p] * inv_1ma;
                         }
                         // gradient terms of backward.rs:453-484, as fused multiply-adds
