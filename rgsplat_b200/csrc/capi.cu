@@ -41,7 +41,8 @@ struct StepHdr {
 struct StepOut {
     uint32_t pairs;
     int overflow;
-    uint32_t pad[2];
+    uint32_t visible;
+    uint32_t pad;
     float losses[MAX_VIEWS];
 };
 
@@ -52,6 +53,7 @@ enum {
     SC_WORK_F = 3,
     SC_WORK_B = 4,
     SC_FINITE = 5,
+    SC_VISIBLE = 6,
     SC_COUNT = 8
 };
 
@@ -386,10 +388,12 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
     cudaStream_t st = ctx->st;
     const size_t S = (size_t)s.n * V;
     uint32_t* sc = ctx->scalars.as<uint32_t>();
-    if (project)
+    if (project) {
+        cudaMemsetAsync(sc + SC_VISIBLE, 0, 4, st);
         launch_project(s.params.as<float4>(), s.n, s.cap, cams_dev, V, ctx->opt.tile_w, ctx->opt.tile_h,
                        ctx->rec.as<float4>(), ctx->cnt.as<uint32_t>(), ctx->tdesc.as<uint2>(), ctx->dkey.as<uint32_t>(),
-                       ctx->ids.as<uint32_t>(), prune ? 1 : 0, st);
+                       ctx->ids.as<uint32_t>(), prune ? 1 : 0, sc + SC_VISIBLE, st);
+    }
     mark(ctx, 1);
     cudaError_t e;
     int which = radix_sort_pairs(ctx->dkey.as<uint32_t>(), ctx->ids.as<uint32_t>(), (uint32_t)S, nullptr, 32, ctx->sort,
@@ -400,9 +404,11 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
     launch_count_scan(order, ctx->cnt.as<uint32_t>(), (uint32_t)S, ctx->block_sums.as<uint32_t>(), sc + SC_PAIRS,
                       bin_grid_blocks(), st);
     if (host_count) {
-        uint32_t K = 0;
+        uint32_t K = 0, vis = 0;
         CK(cudaMemcpyAsync(&K, sc + SC_PAIRS, 4, cudaMemcpyDeviceToHost, st));
+        if (project) CK(cudaMemcpyAsync(&vis, sc + SC_VISIBLE, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        ctx->stats.visible += vis;
         int rc = ensure_pairs(ctx, K);
         if (rc) return rc;
         ctx->stats.pairs += K;
@@ -1168,6 +1174,7 @@ int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], fl
         mark(ctx, 9);
         cudaMemcpyAsync(&ctx->out_h->pairs, sc + SC_PAIRS, 4, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(&ctx->out_h->overflow, sc + SC_OVERFLOW, 4, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(&ctx->out_h->visible, sc + SC_VISIBLE, 4, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(ctx->out_h->losses, losses_dev, sizeof(float) * V, cudaMemcpyDeviceToHost, st);
     }
     cudaGraph_t graph = nullptr;
@@ -1266,6 +1273,7 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
             prof_collect(ctx);
         }
         ctx->stats.pairs = ctx->out_h->pairs;
+        ctx->stats.visible = ctx->out_h->visible;
         if (!ctx->out_h->overflow) {
             if (losses)
                 for (int v = 0; v < V; ++v) losses[v] = ctx->out_h->losses[v];

@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(256) k_project(const float4* __restrict__ para
                                                  const DevCam* __restrict__ cams, int nviews, int tile_w,
                                                  int tile_h, float4* __restrict__ rec, uint32_t* __restrict__ cnt,
                                                  uint2* __restrict__ tdesc, uint32_t* __restrict__ dkey,
-                                                 uint32_t* __restrict__ ids, int prune) {
+                                                 uint32_t* __restrict__ ids, int prune, uint32_t* __restrict__ visible) {
     size_t S = (size_t)n * nviews;
     size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S) return;
@@ -158,17 +158,23 @@ __global__ void __launch_bounds__(256) k_project(const float4* __restrict__ para
         }
     }
     cnt[s] = count;
+    if (count) {
+        // slots with tile pairs, one atomic per group of converged lanes
+        const unsigned m = __activemask();
+        if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(visible, (uint32_t)__popc(m));
+    }
     tdesc[s] = make_uint2((uint32_t)(c.tile_base + cty0 * c.tiles_x + ctx0),
                           (uint32_t)(ctx1 - ctx0) | ((uint32_t)(cty1 - cty0) << 16));
     dkey[s] = __float_as_uint(o.depth);
 }
 
 void launch_project(const float4* params, int n, int cap, const DevCam* cams, int nviews, int tile_w, int tile_h,
-                    float4* rec, uint32_t* cnt, uint2* tdesc, uint32_t* dkey, uint32_t* ids, int prune, cudaStream_t st) {
+                    float4* rec, uint32_t* cnt, uint2* tdesc, uint32_t* dkey, uint32_t* ids, int prune, uint32_t* visible,
+                    cudaStream_t st) {
     size_t S = (size_t)n * nviews;
     if (S == 0) return;
     unsigned blocks = (unsigned)((S + 255) / 256);
-    k_project<<<blocks, 256, 0, st>>>(params, n, cap, cams, nviews, tile_w, tile_h, rec, cnt, tdesc, dkey, ids, prune);
+    k_project<<<blocks, 256, 0, st>>>(params, n, cap, cams, nviews, tile_w, tile_h, rec, cnt, tdesc, dkey, ids, prune, visible);
 }
 
 // ---------------------------------------------------------------------------

@@ -117,9 +117,10 @@ void launch_check_finite(const float4* planes, int n, int cap, int* flag, cudaSt
 // tdesc[s] = (global id of the splat's first CTA tile, width | height << 16 of
 // its CTA-tile rectangle), cnt[s] = its number of CTA tiles, or with prune = 1
 // the number inside the rows' kept spans (tiles.cuh); zero for culled slots.
+// *visible (zeroed by the caller) gains the number of slots with cnt > 0.
 void launch_project(const float4* params, int n, int cap, const DevCam* cams, int nviews,
                     int tile_w, int tile_h, float4* rec, uint32_t* cnt, uint2* tdesc, uint32_t* dkey,
-                    uint32_t* ids, int prune, cudaStream_t st);
+                    uint32_t* ids, int prune, uint32_t* visible, cudaStream_t st);
 void launch_project_wgsl(const float4* params, int n, int cap, const DevCam* cam, int cpu_math,
                          float* splats10, uint32_t* keys, cudaStream_t st);
 void launch_composite_prepare(const float* splats10, int n, const DevCam* cam, int tile_w, int tile_h,
