@@ -78,13 +78,16 @@ __device__ __forceinline__ int stage_batch(const BlendArgs& a, size_t S, uint32_
             const TileTest t = tile_test_setup(A.x, A.y, Q.x, Q.y, Q.z, A.w);
             keep = !tile_rejects(t, x0c, x1c, y0c, y1c);
             if (WMASK && keep) {
-                // the same test per warp: warp ww owns pixel rows [ww*RW, ww*RW + RW)
-                // of the tile, all its columns
-#pragma unroll
-                for (int ww = 0; ww < NW; ++ww) {
-                    const int r0 = ytile + ww * RW;
-                    const int r1 = min(r0 + RW, height) - 1;
-                    if (r0 <= r1 && !tile_rejects(t, x0c, x1c, (float)r0 + 0.5f, (float)r1 + 0.5f)) wm |= 1u << ww;
+                // warp ww owns pixel rows [ww*RW, ww*RW + RW) of the tile: keep the
+                // warps whose rows meet the splat's y-extent (tiles.cuh)
+                float y0, y1;
+                if (splat_y_extent(t, y0, y1)) {
+                    const float lo = (y0 - (float)ytile - 0.5f) / (float)RW, hi = (y1 - (float)ytile - 0.5f) / (float)RW;
+                    const int wlo = (int)fmaxf(ceilf(lo - 1.0f + 1.0f / (float)RW), 0.0f);
+                    const int whi = (int)fminf(floorf(hi), (float)(NW - 1));
+                    wm = whi >= wlo ? ((2u << whi) - (1u << wlo)) : 0u;
+                } else {
+                    wm = (1u << NW) - 1u;
                 }
             }
             if (s_rall) s_rall[j] = make_uint2(__float_as_uint(Q.w), __float_as_uint(K.w));
