@@ -152,6 +152,19 @@ int rgs_render_and_backward_variant(rgs_ctx* ctx, const float* gaussians, size_t
 int rgs_render_color(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, const float bg[3],
                      float* rgb_out);
 
+/* cpu::rasterize (src/cpu/rasterizer.rs:72-192): the forward-only preview
+ * render. Same projection, depth order and 16x16 tile lists as the training
+ * path, but each pixel's colour starts at bg and the splats' weighted colours
+ * are added to it (bg is not scaled by the remaining transmittance,
+ * rasterizer.rs:133); alpha = 1 - T; tiles no splat touches stay
+ * (0, 0, 0, 0). out: w*h*4 floats (RGS_FB_RGBA_F32, Framebuffer::data) or
+ * w*h*4 bytes (RGS_FB_RGBA8_SRGB, Framebuffer::to_u8_srgb, rasterizer.rs:38-48;
+ * converted on the device). */
+#define RGS_FB_RGBA_F32 0
+#define RGS_FB_RGBA8_SRGB 1
+int rgs_rasterize(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, const float bg[3], int format,
+                  void* out);
+
 /* cpu::backward::photometric_loss_grad (src/cpu/backward.rs:646-693). */
 int rgs_photometric_loss_grad(rgs_ctx* ctx, const float* rendered_rgb, const float* target_rgba, uint32_t width,
                               uint32_t height, float lambda, float* loss_out, float* dl_out);

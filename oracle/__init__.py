@@ -165,6 +165,9 @@ def _declare(L: C.CDLL) -> None:
     L.orc_render_and_backward_f.argtypes = [fp, sz, cam, fp, fp, C.c_float, fp, fp, fp, fp, ip, fp, fp]
     L.orc_render_and_backward_d.argtypes = [dp, sz, cam, dp, dp, C.c_double, dp, dp, dp, dp, ip, dp, dp]
     L.orc_render_color_f.argtypes = [fp, sz, cam, fp, fp, fp, ip]
+    L.orc_rasterize_f.argtypes = [fp, sz, cam, fp, fp]
+    L.orc_to_u8_srgb.argtypes = [fp, sz, C.POINTER(C.c_uint8)]
+    L.orc_linear_to_srgb.argtypes = [fp, sz, fp]
     L.orc_photometric_loss_grad_f.argtypes = [fp, fp, C.c_int, C.c_int, C.c_float, fp, fp]
     L.orc_photometric_loss_grad_d.argtypes = [dp, dp, C.c_int, C.c_int, C.c_double, dp, dp]
     L.orc_project_f.argtypes = [fp, sz, cam, ip, fp, ip]
@@ -285,6 +288,31 @@ def render_color(gaussians, camera: Camera, bg=(0.0, 0.0, 0.0)):
     cs = camera_struct(camera)
     _check(lib().orc_render_color_f(_f(g), g.shape[0], C.byref(cs), _f(bgv), _f(rgb), _f(ft), _i(lc)), "render_color")
     return rgb, ft, lc
+
+
+def rasterize(gaussians, camera: Camera, bg=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """``cpu::rasterize`` (src/cpu/rasterizer.rs:72-192) -> Framebuffer RGBA (H, W, 4)."""
+    g = f32(gaussians).reshape(-1, 59)
+    rgba = np.zeros((camera.height, camera.width, 4), np.float32)
+    cs = camera_struct(camera)
+    _check(lib().orc_rasterize_f(_f(g), g.shape[0], C.byref(cs), _f(f32(bg)), _f(rgba)), "rasterize")
+    return rgba
+
+
+def linear_to_srgb(x) -> np.ndarray:
+    """``linear_to_srgb`` (src/cpu/rasterizer.rs:262-269)."""
+    a = f32(np.atleast_1d(x))
+    out = np.zeros_like(a)
+    _check(lib().orc_linear_to_srgb(_f(a), a.size, _f(out)), "linear_to_srgb")
+    return out
+
+
+def to_u8_srgb(rgba) -> np.ndarray:
+    """``Framebuffer::to_u8_srgb`` (src/cpu/rasterizer.rs:38-48)."""
+    a = f32(rgba)
+    out = np.zeros(a.shape, np.uint8)
+    _check(lib().orc_to_u8_srgb(_f(a), a.size, out.ctypes.data_as(C.POINTER(C.c_uint8))), "to_u8_srgb")
+    return out
 
 
 def photometric_loss_grad(rendered, target_rgba, w: int, h: int, lam: float, double=False):

@@ -57,6 +57,22 @@ int orc_render_color_f(const float* g, size_t n, const orc_camera* cam, const fl
     return render_color((const Gaussian<float>*)g, n, c, bg, rgb, final_t, last);
 }
 
+int orc_rasterize_f(const float* g, size_t n, const orc_camera* cam, const float* bg, float* rgba) {
+    Cam<float> c;
+    if (!cam || !make_cam(*cam, c)) return ORC_EINVAL;
+    return rasterize((const Gaussian<float>*)g, n, c, bg, rgba);
+}
+
+int orc_linear_to_srgb(const float* x, size_t n, float* out) {
+    for (size_t i = 0; i < n; ++i) out[i] = fm::linear_to_srgb(x[i]);
+    return ORC_OK;
+}
+
+int orc_to_u8_srgb(const float* rgba, size_t n_values, uint8_t* out) {
+    to_u8_srgb(rgba, n_values, out);
+    return ORC_OK;
+}
+
 int orc_photometric_loss_grad_f(const float* rendered, const float* target, int w, int h, float lambda, float* loss, float* dl) {
     if (w <= 0 || h <= 0) return ORC_EINVAL;
     *loss = photometric_loss_grad(rendered, target, w, h, lambda, dl);

@@ -68,12 +68,9 @@ inline float exp_cr(float x) {
     return (float)exp_core_d((double)x);
 }
 
-inline float log_cr(float x) {
-    if (x != x) return x + x;
-    if (x < 0.0f) return std::numeric_limits<float>::quiet_NaN();
-    if (x == 0.0f) return -std::numeric_limits<float>::infinity();
-    if (x == std::numeric_limits<float>::infinity()) return x;
-    double d = (double)x;  // every positive float is a normal double
+// ln(d) in double for a positive, finite d that came from a float (every
+// positive float is a normal double).
+inline double log_pos_d(double d) {
     uint64_t b = double_to_bits(d);
     int e = (int)((b >> 52) & 0x7ffu) - 1023;
     double m = bits_to_double((b & 0x000fffffffffffffull) | 0x3ff0000000000000ull);  // [1, 2)
@@ -93,8 +90,32 @@ inline float log_cr(float x) {
     P = std::fma(P, z, 2.0 / 3.0);
     double logm = std::fma(s * z, P, 2.0 * s);
     double ef = (double)e;
-    double r = ef * LN2_HI_D + std::fma(ef, LN2_LO_D, logm);
-    return (float)r;
+    return ef * LN2_HI_D + std::fma(ef, LN2_LO_D, logm);
+}
+
+inline float log_cr(float x) {
+    if (x != x) return x + x;
+    if (x < 0.0f) return std::numeric_limits<float>::quiet_NaN();
+    if (x == 0.0f) return -std::numeric_limits<float>::infinity();
+    if (x == std::numeric_limits<float>::infinity()) return x;
+    return (float)log_pos_d((double)x);
+}
+
+// rasterizer.rs:262-269 linear_to_srgb (IEC 61966-2-1). The reference calls
+// f32::powf(x, 1.0 / 2.4); here x^y = exp(y ln x) is evaluated in double and
+// rounded once (correctly rounded except in rare near-halfway cases).
+inline float linear_to_srgb(float x) {
+    if (x <= 0.0031308f) return 12.92f * x;
+    const float y = 1.0f / 2.4f;
+    const float p = (float)exp_core_d((double)y * log_pos_d((double)x));
+    return 1.055f * p - 0.055f;
+}
+
+// Rust `f as u8`: truncate toward zero, saturate, NaN -> 0.
+inline uint8_t as_u8(float f) {
+    if (!(f > 0.0f)) return 0;
+    if (f >= 255.0f) return 255;
+    return (uint8_t)(int)f;
 }
 
 inline float expf_fast(float x) {

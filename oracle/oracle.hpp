@@ -824,6 +824,64 @@ template <class T> inline int render_and_backward(const Gaussian<T>* gs, size_t 
     return ORC_OK;
 }
 
+// cpu::rasterize, src/cpu/rasterizer.rs:72-192: the same projection, depth
+// order and 16x16 tile lists as the training path (project_gaussian,
+// rasterizer.rs:198-257, repeats backward.rs's project), composited per pixel
+// from a colour that STARTS at bg (tile_buf init, :133) with the weighted
+// splat colours added and no bg * T term; alpha = 1 - T (:179). A pixel stops
+// taking splats once T < 1e-4 (:147). Tiles no splat touches keep (0, 0, 0, 0).
+template <class T> inline int rasterize(const Gaussian<T>* gs, size_t n, const Cam<T>& cam, const T bg[3], T* rgba) {
+    Binned<T> B;
+    int rc = project_and_bin(gs, n, cam, B);
+    if (rc) return rc;
+    const int w = cam.w, h = cam.h;
+    const T ATH = Consts<T>::alpha_threshold(), TST = Consts<T>::transmittance_stop(), MA = Consts<T>::max_alpha();
+    std::fill(rgba, rgba + (size_t)w * h * 4, T(0));
+#pragma omp parallel for schedule(dynamic, 4)
+    for (long ti = 0; ti < (long)B.tile_lists.size(); ++ti) {
+        const std::vector<int>& L = B.tile_lists[ti];
+        if (L.empty()) continue;
+        int tx = (int)(ti % B.ntx), ty = (int)(ti / B.ntx);
+        int px0 = tx * TILE_SIZE, py0 = ty * TILE_SIZE;
+        int px1 = std::min(px0 + TILE_SIZE, w), py1 = std::min(py0 + TILE_SIZE, h);
+        for (int py = py0; py < py1; ++py)
+            for (int px = px0; px < px1; ++px) {
+                T t = 1, col[3] = {bg[0], bg[1], bg[2]};
+                for (size_t li = 0; li < L.size(); ++li) {
+                    if (t < TST) break;
+                    const Splat<T>& s = B.splats[L[li]];
+                    T dx = (T)px + T(0.5) - s.sx;
+                    T dy = (T)py + T(0.5) - s.sy;
+                    T a = s.conic[0], b = s.conic[1], c = s.conic[2];
+                    T power = T(-0.5) * (a * dx * dx + T(2) * b * dx * dy + c * dy * dy);
+                    if (power > T(0)) continue;
+                    T alpha = rmin(s.opacity * t_expa(power), MA);
+                    if (alpha < ATH) continue;
+                    T weight = alpha * t;
+                    col[0] += s.color[0] * weight;
+                    col[1] += s.color[1] * weight;
+                    col[2] += s.color[2] * weight;
+                    t *= T(1) - alpha;
+                }
+                size_t pix = (size_t)py * w + px;
+                rgba[pix * 4] = col[0];
+                rgba[pix * 4 + 1] = col[1];
+                rgba[pix * 4 + 2] = col[2];
+                rgba[pix * 4 + 3] = T(1) - t;
+            }
+    }
+    return ORC_OK;
+}
+
+// Framebuffer::to_u8_srgb, rasterizer.rs:38-48: RGB through linear_to_srgb,
+// alpha linear, each clamped to [0, 1], scaled by 255 and cast as u8.
+inline void to_u8_srgb(const float* rgba, size_t n_values, uint8_t* out) {
+    for (size_t i = 0; i < n_values; ++i) {
+        const float v = rclamp(rgba[i], 0.0f, 1.0f);
+        out[i] = i % 4 == 3 ? fm::as_u8(v * 255.0f) : fm::as_u8(fm::linear_to_srgb(v) * 255.0f);
+    }
+}
+
 // backward.rs:152-166
 template <class T> inline int render_color(const Gaussian<T>* gs, size_t n, const Cam<T>& cam, const T bg[3], T* rgb, T* final_t_out, int32_t* last_out) {
     Binned<T> B;

@@ -18,6 +18,7 @@ from .api import (  # noqa: F401
     densify_and_prune,
     estimate_scene_extent,
     photometric_loss_grad,
+    rasterize,
     render_and_backward,
     render_and_backward_variant,
     render_color,

@@ -27,6 +27,8 @@ RGS_NUM_STAGES = 9
 STAGE_NAMES = ("project", "depth_sort", "emit", "tile_sort", "ranges", "forward", "loss", "backward", "geometry_adam")
 RGS_PROJECT_WGSL = 0
 RGS_PROJECT_CPU_MATH = 1
+RGS_FB_RGBA_F32 = 0
+RGS_FB_RGBA8_SRGB = 1
 
 ERROR_NAMES = {
     RGS_ERR_INVALID_ARG: "invalid argument",
@@ -155,6 +157,7 @@ SIGNATURES = {
     "rgs_render_and_backward": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), FP, FP, C.POINTER(rgs_loss_config), FP, FP]),
     "rgs_render_and_backward_variant": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), FP, FP, C.POINTER(rgs_loss_config),
                                                   C.c_int, FP, FP, C.POINTER(rgs_backward_report)]),
+    "rgs_rasterize": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), FP, C.c_int, C.c_void_p]),
     "rgs_render_color": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), FP, FP]),
     "rgs_photometric_loss_grad": (C.c_int, [CTX, FP, FP, C.c_uint32, C.c_uint32, C.c_float, FP, FP]),
     "rgs_photometric_loss_grad_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_float,

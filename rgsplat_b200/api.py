@@ -288,6 +288,22 @@ def render_color(gaussians, camera: Camera, bg=(0.0, 0.0, 0.0), ctx: Context | N
     return out
 
 
+def rasterize(gaussians, camera: Camera, bg=(0.0, 0.0, 0.0), srgb8: bool = False, ctx: Context | None = None) -> np.ndarray:
+    """``cpu::rasterize`` (src/cpu/rasterizer.rs:72-192) -> the Framebuffer's RGBA
+    (H, W, 4) float32, or with srgb8 its ``to_u8_srgb`` bytes (uint8)."""
+    ctx = ctx or default_context()
+    g = _gauss(gaussians)
+    cam = camera_c(camera)
+    if srgb8:
+        out = np.zeros((camera.height, camera.width, 4), np.uint8)
+        fmt = L.RGS_FB_RGBA8_SRGB
+    else:
+        out = np.zeros((camera.height, camera.width, 4), np.float32)
+        fmt = L.RGS_FB_RGBA_F32
+    ctx.check(ctx.lib.rgs_rasterize(ctx.handle, _fp(g), g.shape[0], C.byref(cam), _fp(_f32(bg)), fmt, out.ctypes.data))
+    return out
+
+
 def photometric_loss_grad(rendered, target_rgba, w: int, h: int, lam: float, ctx: Context | None = None):
     """``photometric_loss_grad`` (src/cpu/backward.rs:646-693) -> (loss, dL/dpixel (w*h*3,))."""
     ctx = ctx or default_context()

@@ -157,7 +157,9 @@ __global__ void __launch_bounds__(TW * TH / PPT) k_blend_fwd(BlendArgs a) {
         for (int p = 0; p < PPT; ++p) {
             pyc[p] = (float)(py0 + p) + 0.5f;
             T[p] = 1.0f;
-            C0[p] = C1[p] = C2[p] = 0.0f;
+            C0[p] = a.bg_start ? a.bg[0] : 0.0f;
+            C1[p] = a.bg_start ? a.bg[1] : 0.0f;
+            C2[p] = a.bg_start ? a.bg[2] : 0.0f;
             last[p] = -1;
             done[p] = !(px < c.width && py0 + p < c.height);
             all_done &= done[p];
@@ -218,9 +220,9 @@ __global__ void __launch_bounds__(TW * TH / PPT) k_blend_fwd(BlendArgs a) {
                 // forward_pass skips tiles whose list is empty, leaving their pixels
                 // at 0 rather than bg (src/cpu/backward.rs:313-315, 124)
                 const bool black = a.empty_tile_black && !seen[p];
-                a.rgb[pix * 3 + 0] = black ? 0.0f : C0[p] + T[p] * a.bg[0];
-                a.rgb[pix * 3 + 1] = black ? 0.0f : C1[p] + T[p] * a.bg[1];
-                a.rgb[pix * 3 + 2] = black ? 0.0f : C2[p] + T[p] * a.bg[2];
+                a.rgb[pix * 3 + 0] = black ? 0.0f : a.bg_start ? C0[p] : C0[p] + T[p] * a.bg[0];
+                a.rgb[pix * 3 + 1] = black ? 0.0f : a.bg_start ? C1[p] : C1[p] + T[p] * a.bg[1];
+                a.rgb[pix * 3 + 2] = black ? 0.0f : a.bg_start ? C2[p] : C2[p] + T[p] * a.bg[2];
                 a.final_t[pix] = T[p];
                 a.last[pix] = last[p];
             }

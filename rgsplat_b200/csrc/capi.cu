@@ -472,6 +472,7 @@ BlendArgs blend_args(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, cons
     a.empty_tile_black = 1;
     a.pixels_per_thread = ctx->opt.pixels_per_thread;
     a.tstore = nullptr;
+    a.bg_start = 0;
     return a;
 }
 
@@ -501,7 +502,8 @@ struct BwdStudy {
 // Forward + loss + backward + geometry of one view (the plain path).
 // grads: accumulate (v > 0) or overwrite into s.grads; loss_out may be null.
 int run_view_plain(rgs_ctx* ctx, Scene& s, const DevCam& dc_in, const float* target_dev, const float bg[3], float lambda,
-                   bool do_backward, bool accumulate, float* loss_out, float* rgb_host, BwdStudy* study = nullptr) {
+                   bool do_backward, bool accumulate, float* loss_out, float* rgb_host, BwdStudy* study = nullptr,
+                   bool bg_start = false) {
     cudaStream_t st = ctx->st;
     DevCam dc = dc_in;
     dc.target = target_dev;
@@ -515,6 +517,7 @@ int run_view_plain(rgs_ctx* ctx, Scene& s, const DevCam& dc_in, const float* tar
     Binned b;
     if ((rc = bin_batch(ctx, s, cams_dev, 1, tiles, true, b, true, zero_bg(bg)))) return rc;
     BlendArgs fa = blend_args(ctx, s, cams_dev, 1, nullptr, tiles, b, bg, true);
+    fa.bg_start = bg_start ? 1 : 0;
     if (study) {
         // blend state: final T + last contributor per pixel, plus (store-all)
         // T per (tile-list position, tile pixel)
@@ -815,6 +818,30 @@ int rgs_render_color(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_c
     if ((rc = check_finite(ctx, s))) return rc;
     ctx->stats = rgs_stats{};
     return run_view_plain(ctx, s, dc, nullptr, bg, 0.0f, false, false, nullptr, rgb_out);
+}
+
+int rgs_rasterize(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, const float bg[3], int format,
+                  void* out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!camera || !bg || !out || (n && !gaussians)) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
+    if (format != RGS_FB_RGBA_F32 && format != RGS_FB_RGBA8_SRGB) return fail(ctx, RGS_ERR_INVALID_ARG, "unknown framebuffer format");
+    DevCam dc;
+    if ((rc = make_devcam(ctx, *camera, dc))) return rc;
+    Scene& s = ctx->sc;
+    if ((rc = upload_gaussians(ctx, s, gaussians, n))) return rc;
+    if ((rc = check_finite(ctx, s))) return rc;
+    ctx->stats = rgs_stats{};
+    if ((rc = run_view_plain(ctx, s, dc, nullptr, bg, 0.0f, false, false, nullptr, nullptr, nullptr, true))) return rc;
+    const size_t px = (size_t)camera->width * camera->height;
+    const size_t bytes = px * (format == RGS_FB_RGBA8_SRGB ? 4 : 16);
+    CK(ctx->stage_a.ensure(std::max<size_t>(bytes, 16)));
+    launch_pack_framebuffer(ctx->rgb.as<float>(), ctx->final_t.as<float>(), px, format == RGS_FB_RGBA8_SRGB ? 1 : 0,
+                            ctx->stage_a.p, ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, ctx->stage_a.p, bytes, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return RGS_OK;
 }
 
 int rgs_photometric_loss_grad(rgs_ctx* ctx, const float* rendered_rgb, const float* target_rgba, uint32_t width,

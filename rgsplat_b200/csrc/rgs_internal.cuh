@@ -170,10 +170,15 @@ struct BlendArgs {
     int empty_tile_black;          // pixels of empty reference tiles render 0, not bg
     int pixels_per_thread;         // 1 or 2 vertically adjacent pixels per thread
     float* tstore;                 // store-all variant only: T per (list position, tile pixel)
+    int bg_start;                  // preview compositing (rasterizer.rs:133): colour starts at bg and
+                                   // the output is that sum, bg not scaled by the final T
 };
 void launch_blend_forward(const BlendArgs& a, int tile_w, int tile_h, int batch, cudaStream_t st);
 void launch_blend_backward(const BlendArgs& a, int tile_w, int tile_h, int batch, cudaStream_t st);
 void launch_blend_store_all(const BlendArgs& a, bool fwd, cudaStream_t st);
+
+// raster.cu: preview framebuffer (colour, 1 - T) as RGBA f32 or sRGB RGBA8.
+void launch_pack_framebuffer(const float* rgb, const float* final_t, size_t npix, int srgb8, void* out, cudaStream_t st);
 
 // loss.cu
 void launch_loss(const DevCam* cams, int nviews, int total_blocks, const float* rgb, float lambda,

@@ -56,14 +56,10 @@ __device__ __forceinline__ float exp_cr(float x) {
     return __double2float_rn(exp_core_d((double)x));
 }
 
-__device__ __forceinline__ float log_cr(float x) {
-    if (x != x) return x + x;
-    if (x < 0.0f) return __int_as_float(0x7fc00000);
-    if (x == 0.0f) return __int_as_float(0xff800000);
-    if (x == __int_as_float(0x7f800000)) return x;
+// ln(d) in double for a positive, finite d that came from a float.
+__device__ __forceinline__ double log_pos_d(double d) {
     const double LN2_HI = 6.93147180369123816490e-01;
     const double LN2_LO = 1.90821492927058770002e-10;
-    double d = (double)x;
     unsigned long long b = (unsigned long long)__double_as_longlong(d);
     int e = (int)((b >> 52) & 0x7ffull) - 1023;
     double m = __longlong_as_double((long long)((b & 0x000fffffffffffffull) | 0x3ff0000000000000ull));
@@ -83,8 +79,31 @@ __device__ __forceinline__ float log_cr(float x) {
     P = fma(P, z, 2.0 / 3.0);
     double logm = fma(s * z, P, 2.0 * s);
     double ef = (double)e;
-    double r = ef * LN2_HI + fma(ef, LN2_LO, logm);
-    return __double2float_rn(r);
+    return ef * LN2_HI + fma(ef, LN2_LO, logm);
+}
+
+__device__ __forceinline__ float log_cr(float x) {
+    if (x != x) return x + x;
+    if (x < 0.0f) return __int_as_float(0x7fc00000);
+    if (x == 0.0f) return __int_as_float(0xff800000);
+    if (x == __int_as_float(0x7f800000)) return x;
+    return __double2float_rn(log_pos_d((double)x));
+}
+
+// linear_to_srgb (src/cpu/rasterizer.rs:262-269, IEC 61966-2-1): powf(x, 1/2.4)
+// evaluated as exp(y ln x) in double and rounded once.
+__device__ __forceinline__ float linear_to_srgb(float x) {
+    if (x <= 0.0031308f) return 12.92f * x;
+    const float y = 1.0f / 2.4f;
+    const float p = __double2float_rn(exp_core_d((double)y * log_pos_d((double)x)));
+    return 1.055f * p - 0.055f;
+}
+
+// Rust `f as u8`: truncate toward zero, saturate, NaN -> 0.
+__device__ __forceinline__ unsigned char as_u8(float f) {
+    if (!(f > 0.0f)) return 0;
+    if (f >= 255.0f) return 255;
+    return (unsigned char)(int)f;
 }
 
 __device__ __forceinline__ float expf_fast(float x) {

@@ -303,3 +303,15 @@ def test_training_reduces_photometric_loss_gpu(ctx):
     img = R.render_color(gs, cam, ctx=ctx)
     for ch in range(3):
         assert abs(img[h // 2, w // 2, ch] - target[0, 0, ch]) < 0.15
+
+
+# ---- cpu::rasterize preview (src/cpu/rasterizer.rs:72-192) ------------------------
+@pytest.mark.parametrize("bg", [(0.0, 0.0, 0.0), (0.2, 0.5, 0.9)])
+def test_rasterize_matches_oracle(ctx, bg):
+    g, cam, _ = small_scene(seed=12, w=200, h=136)
+    fb = R.rasterize(g, cam, bg, ctx=ctx)
+    ofb = O.rasterize(g, cam, bg)
+    assert np.array_equal(fb.reshape(-1).view(np.uint32), ofb.reshape(-1).view(np.uint32)), \
+        f"max diff {np.abs(fb - ofb).max()}"
+    u8 = R.rasterize(g, cam, bg, srgb8=True, ctx=ctx)
+    assert np.array_equal(u8, O.to_u8_srgb(ofb))

@@ -260,3 +260,35 @@ def test_exp_edge_cases():
     for x in (-103.0, -90.0, -87.5, 88.7, -1e-30, 1e-30):
         xf = float(np.float32(x))
         assert O.expf(xf) == np.float32(math.exp(xf))
+
+
+def test_linear_srgb():
+    """src/cpu/rasterizer.rs:275-281 (test_linear_srgb)."""
+    v = O.linear_to_srgb([0.0, 1.0, 0.5])
+    assert abs(v[0] - 0.0) < 1e-6
+    assert abs(v[1] - 1.0) < 1e-6
+    assert v[2] > 0.5
+
+
+def test_rasterize_preview_semantics():
+    """rasterizer.rs:72-192: colour starts at bg (not bg * T), alpha = 1 - T,
+    tiles no splat touches stay (0, 0, 0, 0)."""
+    from tests import refcases as RC
+
+    cam = O.identity_camera(48, 48)
+    g = RC.gaussian_new([0.0, 0.0, 2.0])
+    g[3] = RC.logit(0.9)
+    g[8:11] = -2.5
+    bg = (0.2, 0.3, 0.4)
+    fb = O.rasterize(g[None, :], cam, bg)
+    rgb, ft, _ = O.render_color(g[None, :], cam, bg)
+    c = fb[24, 24]
+    assert 0.0 < c[3] <= 0.99
+    # same splat colour sum as the training forward, bg added unscaled
+    col = rgb[24, 24] - ft[24, 24] * np.array(bg, np.float32)
+    assert np.allclose(c[:3], col + np.array(bg, np.float32), atol=1e-6)
+    assert abs(c[3] - (1.0 - ft[24, 24])) < 1e-7
+    # a corner tile far from the splat has an empty list
+    assert np.all(fb[0:16, 0:16] == 0.0) or np.all(fb[32:48, 32:48] == 0.0)
+    u8 = O.to_u8_srgb(fb)
+    assert u8.dtype == np.uint8 and u8[24, 24, 3] == int(min(max(c[3], 0.0), 1.0) * 255.0)
