@@ -170,17 +170,24 @@ int rgs_photometric_loss_grad(rgs_ctx* ctx, const float* rendered_rgb, const flo
                               uint32_t height, float lambda, float* loss_out, float* dl_out);
 
 /* No counterpart in the reference. rgs_photometric_loss_grad on caller-owned
- * DEVICE buffers for callers that cannot allocate device memory: it allocates
- * nothing (no context, no cudaMalloc) and keeps its scratch (view descriptor
- * plus two floats per 32x32 loss block) in a static device array of
- * 256 + RGS_NOALLOC_MAX_LOSS_BLOCKS * 8 bytes (128.25 KiB) per device, so
- * images are limited to RGS_NOALLOC_MAX_LOSS_BLOCKS loss blocks (4096x4096
- * pixels); larger ones return RGS_ERR_CAPACITY. rendered_rgb: w*h*3,
- * target_rgba: w*h*4, dl_out: w*h*3, loss_out: 1 float, all on `device`.
- * Work is enqueued on `cuda_stream` (NULL = legacy default stream) and the
- * call returns without synchronising. Calls that overlap on one device share
- * the scratch and race: serialise them. On failure a message is written to
- * err (err_len bytes, may be NULL). */
+ * DEVICE buffers, for callers that must not allocate device memory: a host
+ * application or framework that owns every byte of the GPU through its own
+ * pool (a cudaMalloc behind its back can fail or fragment its budget), or a
+ * latency-critical path where cudaMalloc's implicit device synchronisation is
+ * not acceptable. It needs no context and allocates nothing; its scratch (view
+ * descriptor plus two floats per 32x32 loss block) is a static device array
+ * of 256 + RGS_NOALLOC_MAX_LOSS_BLOCKS * 8 bytes (128.25 KiB) that every GPU
+ * loading the library holds until the process exits. Images over
+ * RGS_NOALLOC_MAX_LOSS_BLOCKS loss blocks (4096x4096 pixels) return
+ * RGS_ERR_CAPACITY. rendered_rgb: w*h*3, target_rgba: w*h*4, dl_out: w*h*3,
+ * loss_out: 1 float, all on `device`. Work is enqueued on `cuda_stream`
+ * (NULL = legacy default stream) and the call returns without synchronising.
+ * The first call on a device also sets that device up (looks up the scratch
+ * array's device address and sets the loss kernel's shared-memory limit), so
+ * make that first call before any stream capture on the device. Every call
+ * reuses the same array, which keeps the previous call's contents; calls that
+ * overlap on one device race on it: serialise them. On failure a message is
+ * written to err (err_len bytes, may be NULL). */
 #define RGS_NOALLOC_MAX_LOSS_BLOCKS 16384
 int rgs_photometric_loss_grad_noalloc(int device, const float* rendered_rgb, const float* target_rgba,
                                       uint32_t width, uint32_t height, float lambda, float* loss_out,

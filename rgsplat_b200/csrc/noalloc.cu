@@ -1,20 +1,25 @@
 // noalloc.cu -- rgs_photometric_loss_grad_noalloc: the photometric loss and
 // dL/dpixel on caller-owned device buffers, with no device allocation at all.
+// It is for callers that must not allocate device memory themselves or through
+// this library: applications whose own pool owns the whole GPU, and paths that
+// cannot afford cudaMalloc's implicit synchronisation.
 //
 // Everything the loss kernels need besides the caller's buffers lives in one
 // file-scope static __device__ array: a 256-byte header holding the view
 // descriptor (DevCam) and then two floats (L1 sum, SSIM sum) per 32x32 loss
-// block. Its address is taken with cudaGetSymbolAddress once per device, with
-// that device current, the first time the device is used. The kernels are the
-// ones rgs_photometric_loss_grad runs (loss.cu); only where their scratch
-// lives differs.
+// block. Host code cannot use the array's name as a device address, so the
+// address is looked up with cudaGetSymbolAddress, with the device current,
+// on the first call on each device (that first call also sets the loss
+// kernel's shared-memory limit; it should come before any stream capture).
+// The kernels are the ones rgs_photometric_loss_grad runs (loss.cu); only
+// where their scratch lives differs.
 //
-// Nothing in the scratch has to start at zero: the header is written by a
-// one-thread kernel on the caller's stream before the loss kernels, and every
-// loss block writes its own partial-sum pair before the per-view finalize
-// reads it. Calls that overlap on one device (two host threads, or two
-// streams with work in flight at once) share the scratch and race; callers
-// serialise them.
+// The array keeps whatever the previous call left in it, and nothing in it has
+// to start at zero: the header is written by a one-thread kernel on the
+// caller's stream before the loss kernels, and every loss block writes its own
+// partial-sum pair before the per-view finalize reads it. Calls that overlap
+// on one device (two host threads, or two streams with work in flight at once)
+// share the array and race; callers serialise them.
 #include <mutex>
 
 #include "rgs_internal.cuh"

@@ -1,8 +1,13 @@
 """rgs_photometric_loss_grad_noalloc against rgs_photometric_loss_grad.
 
-The no-allocation variant runs the same loss kernels on caller-owned device
-buffers with its scratch in a static device array, so its loss and dL/dpixel
-must equal the context entry point's bit for bit, call after call.
+The no-allocation variant exists for callers that must not allocate device
+memory (an application whose own pool owns the GPU, or a latency-critical
+path that cannot take cudaMalloc's implicit synchronisation). It runs the
+same loss kernels on the caller's device buffers with its scratch in a static
+device array that every call reuses, so its loss and dL/dpixel must equal the
+context entry point's bit for bit on two calls in a row. This file is
+collected last so a run that stops at its first failure has run everything
+else first; it also passes on its own in a fresh process.
 """
 import ctypes as C
 
