@@ -43,6 +43,8 @@ extern "C" {
 #define RGS_ERR_SINGULAR_CAMERA (-5)
 #define RGS_ERR_CAPACITY (-6)
 #define RGS_ERR_NO_DEVICE (-7)
+#define RGS_ERR_IO (-8)     /* a file could not be opened, read or written */
+#define RGS_ERR_FORMAT (-9) /* a model file is not one the reader accepts */
 
 #define RGS_GAUSSIAN_FLOATS 59
 #define RGS_GRAD_FLOATS 60
@@ -221,6 +223,25 @@ int rgs_project(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera
  * conic, T < 1e-4 skip) on the GPU. rgb_out: w*h*3. */
 int rgs_gpu_render(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, int mode,
                    const float bg[3], float* rgb_out);
+
+/* ---- model files: io::ply (src/io/ply.rs:35-303) --------------------------
+ * save_ply writes the binary little-endian 3DGS layout (62 f32 per vertex,
+ * ply.rs:35-104); save_splat the lossy 32-byte display records (position,
+ * exp(log_scale), RGBA bytes from the DC colour and sigmoid(opacity),
+ * quaternion bytes, ply.rs:253-285); both create the parent directory.
+ * load_ply accepts binary LE / BE and ASCII with properties in any order,
+ * decoding each by its byte width as the reference does (ply.rs:116-252).
+ * The records are packed / unpacked on the device. rgs_load_ply fills up to
+ * `cap` records (n * 59 floats); with out == NULL or cap too small it sets
+ * *n_out to the file's vertex count and returns RGS_ERR_CAPACITY. */
+int rgs_save_ply(rgs_ctx* ctx, const float* gaussians, size_t n, const char* path);
+int rgs_save_splat(rgs_ctx* ctx, const float* gaussians, size_t n, const char* path);
+int rgs_load_ply(rgs_ctx* ctx, const char* path, float* out, size_t cap, size_t* n_out);
+/* The trainer's Gaussians straight from / into device memory; loading resets
+ * the Adam state like rgs_trainer_set_gaussians. */
+int rgs_trainer_save_ply(rgs_ctx* ctx, const char* path);
+int rgs_trainer_save_splat(rgs_ctx* ctx, const char* path);
+int rgs_trainer_load_ply(rgs_ctx* ctx, const char* path, size_t* n_out);
 
 /* ---- device-resident trainer (the training loop of src/pipeline/mod.rs:203-265) */
 

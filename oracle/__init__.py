@@ -168,6 +168,12 @@ def _declare(L: C.CDLL) -> None:
     L.orc_rasterize_f.argtypes = [fp, sz, cam, fp, fp]
     L.orc_to_u8_srgb.argtypes = [fp, sz, C.POINTER(C.c_uint8)]
     L.orc_linear_to_srgb.argtypes = [fp, sz, fp]
+    u8p = C.POINTER(C.c_uint8)
+    L.orc_save_ply.argtypes = [fp, sz, u8p, sz]
+    L.orc_save_ply.restype = C.c_long
+    L.orc_save_splat.argtypes = [fp, sz, u8p, sz]
+    L.orc_save_splat.restype = C.c_long
+    L.orc_load_ply.argtypes = [u8p, sz, fp, sz, C.POINTER(C.c_size_t)]
     L.orc_photometric_loss_grad_f.argtypes = [fp, fp, C.c_int, C.c_int, C.c_float, fp, fp]
     L.orc_photometric_loss_grad_d.argtypes = [dp, dp, C.c_int, C.c_int, C.c_double, dp, dp]
     L.orc_project_f.argtypes = [fp, sz, cam, ip, fp, ip]
@@ -304,6 +310,35 @@ def linear_to_srgb(x) -> np.ndarray:
     a = f32(np.atleast_1d(x))
     out = np.zeros_like(a)
     _check(lib().orc_linear_to_srgb(_f(a), a.size, _f(out)), "linear_to_srgb")
+    return out
+
+
+def _encode(fn, gaussians) -> bytes:
+    g = f32(gaussians).reshape(-1, 59)
+    size = fn(_f(g), g.shape[0], None, 0)
+    buf = np.zeros(size, np.uint8)
+    fn(_f(g), g.shape[0], buf.ctypes.data_as(C.POINTER(C.c_uint8)), size)
+    return buf.tobytes()
+
+
+def save_ply_bytes(gaussians) -> bytes:
+    """``io::ply::save_ply`` (src/io/ply.rs:35-104) as the file's bytes."""
+    return _encode(lib().orc_save_ply, gaussians)
+
+
+def save_splat_bytes(gaussians) -> bytes:
+    """``io::ply::save_splat`` (src/io/ply.rs:253-285) as the file's bytes."""
+    return _encode(lib().orc_save_splat, gaussians)
+
+
+def load_ply_bytes(data: bytes) -> np.ndarray:
+    """``io::ply::load_ply`` (src/io/ply.rs:116-193) of a file's bytes -> (N, 59)."""
+    buf = np.frombuffer(data, np.uint8)
+    n = C.c_size_t(0)
+    p = buf.ctypes.data_as(C.POINTER(C.c_uint8))
+    _check(lib().orc_load_ply(p, buf.size, None, 0, C.byref(n)), "load_ply")
+    out = np.zeros((n.value, 59), np.float32)
+    _check(lib().orc_load_ply(p, buf.size, _f(out), n.value, C.byref(n)), "load_ply")
     return out
 
 

@@ -6,6 +6,7 @@
 #include <omp.h>
 
 #include "oracle.hpp"
+#include "ply.hpp"
 
 namespace orc {
 int g_libm_math = 0;
@@ -70,6 +71,28 @@ int orc_linear_to_srgb(const float* x, size_t n, float* out) {
 
 int orc_to_u8_srgb(const float* rgba, size_t n_values, uint8_t* out) {
     to_u8_srgb(rgba, n_values, out);
+    return ORC_OK;
+}
+
+// io::ply (src/io/ply.rs): encoders return the byte count and fill `out` when
+// it holds at least that many bytes; the decoder fills up to `cap` records.
+long orc_save_ply(const float* g, size_t n, uint8_t* out, size_t cap) {
+    auto b = ply::save_ply(g, n);
+    if (out && cap >= b.size()) std::memcpy(out, b.data(), b.size());
+    return (long)b.size();
+}
+long orc_save_splat(const float* g, size_t n, uint8_t* out, size_t cap) {
+    auto b = ply::save_splat(g, n);
+    if (out && cap >= b.size()) std::memcpy(out, b.data(), b.size());
+    return (long)b.size();
+}
+int orc_load_ply(const uint8_t* data, size_t size, float* out, size_t cap, size_t* n_out) {
+    std::vector<float> v;
+    int rc = ply::load_ply(data, size, v);
+    if (rc) return rc;
+    const size_t n = v.size() / 59;
+    *n_out = n;
+    if (out && cap >= n) std::memcpy(out, v.data(), v.size() * 4);
     return ORC_OK;
 }
 

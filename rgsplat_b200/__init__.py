@@ -19,6 +19,9 @@ from .api import (  # noqa: F401
     estimate_scene_extent,
     photometric_loss_grad,
     rasterize,
+    load_ply,
+    save_ply,
+    save_splat,
     render_and_backward,
     render_and_backward_variant,
     render_color,

@@ -20,6 +20,8 @@ RGS_ERR_NONFINITE = -4
 RGS_ERR_SINGULAR_CAMERA = -5
 RGS_ERR_CAPACITY = -6
 RGS_ERR_NO_DEVICE = -7
+RGS_ERR_IO = -8
+RGS_ERR_FORMAT = -9
 
 RGS_STEP_PLAIN = 0
 RGS_STEP_BATCHED = 1
@@ -38,6 +40,8 @@ ERROR_NAMES = {
     RGS_ERR_SINGULAR_CAMERA: "singular camera",
     RGS_ERR_CAPACITY: "capacity exceeded",
     RGS_ERR_NO_DEVICE: "no CUDA device",
+    RGS_ERR_IO: "file error",
+    RGS_ERR_FORMAT: "unsupported model file",
 }
 
 
@@ -167,6 +171,12 @@ SIGNATURES = {
     "rgs_reset_opacities": (C.c_int, [CTX, FP, C.c_size_t]),
     "rgs_project": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), C.c_int, C.POINTER(rgs_splat_info_2d), U32P]),
     "rgs_gpu_render": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), C.c_int, FP, FP]),
+    "rgs_save_ply": (C.c_int, [CTX, FP, C.c_size_t, C.c_char_p]),
+    "rgs_save_splat": (C.c_int, [CTX, FP, C.c_size_t, C.c_char_p]),
+    "rgs_load_ply": (C.c_int, [CTX, C.c_char_p, FP, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "rgs_trainer_save_ply": (C.c_int, [CTX, C.c_char_p]),
+    "rgs_trainer_save_splat": (C.c_int, [CTX, C.c_char_p]),
+    "rgs_trainer_load_ply": (C.c_int, [CTX, C.c_char_p, C.POINTER(C.c_size_t)]),
     "rgs_trainer_set_gaussians": (C.c_int, [CTX, FP, C.c_size_t]),
     "rgs_trainer_count": (C.c_int, [CTX, C.POINTER(C.c_size_t)]),
     "rgs_trainer_get_gaussians": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(C.c_size_t)]),

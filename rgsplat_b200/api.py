@@ -16,6 +16,7 @@ panics (NaN depth, singular camera) these functions raise ``RgsError``.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import threading
 from dataclasses import dataclass, field
 from typing import Sequence
@@ -304,6 +305,33 @@ def rasterize(gaussians, camera: Camera, bg=(0.0, 0.0, 0.0), srgb8: bool = False
     return out
 
 
+def save_ply(gaussians, path, ctx: Context | None = None) -> None:
+    """``io::ply::save_ply`` (src/io/ply.rs:35-104): binary little-endian 3DGS .ply."""
+    ctx = ctx or default_context()
+    g = _gauss(gaussians)
+    ctx.check(ctx.lib.rgs_save_ply(ctx.handle, _fp(g), g.shape[0], os.fsencode(path)))
+
+
+def save_splat(gaussians, path, ctx: Context | None = None) -> None:
+    """``io::ply::save_splat`` (src/io/ply.rs:253-285): 32-byte .splat records."""
+    ctx = ctx or default_context()
+    g = _gauss(gaussians)
+    ctx.check(ctx.lib.rgs_save_splat(ctx.handle, _fp(g), g.shape[0], os.fsencode(path)))
+
+
+def load_ply(path, ctx: Context | None = None) -> np.ndarray:
+    """``io::ply::load_ply`` (src/io/ply.rs:116-193) -> (N, 59) Gaussians."""
+    ctx = ctx or default_context()
+    n = C.c_size_t(0)
+    p = os.fsencode(path)
+    rc = ctx.lib.rgs_load_ply(ctx.handle, p, None, 0, C.byref(n))
+    if rc not in (L.RGS_OK, L.RGS_ERR_CAPACITY):
+        ctx.check(rc)
+    out = np.zeros((max(n.value, 1), GAUSSIAN_FLOATS), np.float32)
+    ctx.check(ctx.lib.rgs_load_ply(ctx.handle, p, _fp(out), out.shape[0], C.byref(n)))
+    return out[: n.value]
+
+
 def photometric_loss_grad(rendered, target_rgba, w: int, h: int, lam: float, ctx: Context | None = None):
     """``photometric_loss_grad`` (src/cpu/backward.rs:646-693) -> (loss, dL/dpixel (w*h*3,))."""
     ctx = ctx or default_context()
@@ -456,6 +484,21 @@ class Trainer:
         self.ctx.check(self.lib.rgs_trainer_step(self.ctx.handle, v.ctypes.data_as(L.U32P), v.size, _fp(_f32(bg)), C.byref(lc),
                                                  C.byref(tc), int(mode), _fp(losses)))
         return losses[: v.size]
+
+    def save_ply(self, path) -> None:
+        """The device-resident Gaussians as a 3DGS .ply (io::ply::save_ply)."""
+        self.ctx.check(self.lib.rgs_trainer_save_ply(self.ctx.handle, os.fsencode(path)))
+
+    def save_splat(self, path) -> None:
+        """The device-resident Gaussians as .splat records (io::ply::save_splat)."""
+        self.ctx.check(self.lib.rgs_trainer_save_splat(self.ctx.handle, os.fsencode(path)))
+
+    def load_ply(self, path) -> int:
+        """Replace the Gaussians with a .ply file's (decoded on the device); the
+        Adam state starts afresh. Returns the count."""
+        n = C.c_size_t(0)
+        self.ctx.check(self.lib.rgs_trainer_load_ply(self.ctx.handle, os.fsencode(path), C.byref(n)))
+        return int(n.value)
 
     def step_host_targets(self, views: Sequence[int], target_ptrs: Sequence[int], bg=(0.0, 0.0, 0.0),
                           loss_cfg: LossConfig | None = None, train_cfg: TrainConfig | None = None) -> np.ndarray:

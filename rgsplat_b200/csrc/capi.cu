@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <filesystem>
 #include <string>
 #include <vector>
 
@@ -1028,22 +1029,19 @@ int rgs_gpu_render(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_cam
 // ===========================================================================
 // device-resident trainer
 // ===========================================================================
+}  // extern "C"
+namespace {
+int fresh_adam_state(rgs_ctx* ctx, Scene& s);
+}
+extern "C" {
+
 int rgs_trainer_set_gaussians(rgs_ctx* ctx, const float* gaussians, size_t n) {
     int rc = check_ctx(ctx);
     if (rc) return rc;
     if (n && !gaussians) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
     Scene& s = ctx->tr;
     if ((rc = upload_gaussians(ctx, s, gaussians, n))) return rc;
-    if ((rc = check_finite(ctx, s))) return rc;
-    if ((rc = ensure_moments(ctx, s, std::max<int>((int)n, 1)))) return rc;
-    CK(cudaMemsetAsync(s.m1.p, 0, (size_t)s.mcap * NPL * 16, ctx->st));
-    CK(cudaMemsetAsync(s.m2.p, 0, (size_t)s.mcap * NPL * 16, ctx->st));
-    CK(cudaMemsetAsync(s.accum.p, 0, (size_t)s.mcap * 4, ctx->st));
-    CK(cudaMemsetAsync(s.denom.p, 0, (size_t)s.mcap * 4, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
-    s.mlen = (int)n;
-    s.t = 0;
-    return RGS_OK;
+    return fresh_adam_state(ctx, s);
 }
 
 int rgs_trainer_count(rgs_ctx* ctx, size_t* n) {
@@ -1095,6 +1093,87 @@ int rgs_trainer_set_target(rgs_ctx* ctx, size_t index, const float* target_rgba)
 }  // extern "C"
 
 namespace {
+
+// After new Gaussians arrived in s.params: reject non-finite ones and start
+// from AdamState::new (zero moments, accumulators and step count).
+int fresh_adam_state(rgs_ctx* ctx, Scene& s) {
+    int rc = check_finite(ctx, s);
+    if (rc) return rc;
+    if ((rc = ensure_moments(ctx, s, std::max<int>(s.n, 1)))) return rc;
+    CK(cudaMemsetAsync(s.m1.p, 0, (size_t)s.mcap * NPL * 16, ctx->st));
+    CK(cudaMemsetAsync(s.m2.p, 0, (size_t)s.mcap * NPL * 16, ctx->st));
+    CK(cudaMemsetAsync(s.accum.p, 0, (size_t)s.mcap * 4, ctx->st));
+    CK(cudaMemsetAsync(s.denom.p, 0, (size_t)s.mcap * 4, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    s.mlen = s.n;
+    s.t = 0;
+    return RGS_OK;
+}
+
+// ---- io::ply (src/io/ply.rs): files <-> device planes -----------------------
+int write_file(rgs_ctx* ctx, const char* path, const std::string& head, const void* body, size_t body_bytes) {
+    // save_ply / save_splat create the parent directory first (ply.rs:36-38, 254-256)
+    std::error_code ec;
+    const std::filesystem::path fp(path);
+    if (fp.has_parent_path()) std::filesystem::create_directories(fp.parent_path(), ec);
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(ctx, RGS_ERR_IO, std::string("creating ") + path);
+    bool ok = head.empty() || std::fwrite(head.data(), 1, head.size(), f) == head.size();
+    ok = ok && (body_bytes == 0 || std::fwrite(body, 1, body_bytes, f) == body_bytes);
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? RGS_OK : fail(ctx, RGS_ERR_IO, std::string("writing ") + path);
+}
+
+int read_file(rgs_ctx* ctx, const char* path, std::vector<uint8_t>& d) {
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(ctx, RGS_ERR_IO, std::string("opening ") + path);
+    d.clear();
+    uint8_t buf[1 << 16];
+    size_t got;
+    while ((got = std::fread(buf, 1, sizeof buf, f)) > 0) d.insert(d.end(), buf, buf + got);
+    const bool bad = std::ferror(f) != 0;
+    std::fclose(f);
+    return bad ? fail(ctx, RGS_ERR_IO, std::string("reading ") + path) : RGS_OK;
+}
+
+// The Gaussians of `s` -> the file of save_ply (ply == true) or save_splat.
+int save_model(rgs_ctx* ctx, Scene& s, const char* path, bool ply) {
+    const size_t n = (size_t)s.n;
+    const size_t bytes = n * (ply ? 62 * 4 : 32);
+    CK(ctx->stage_b.ensure(std::max<size_t>(bytes, 16)));
+    if (ply) launch_pack_ply(s.params.as<float4>(), s.n, s.cap, ctx->stage_b.as<float>(), ctx->st);
+    else launch_pack_splat(s.params.as<float4>(), s.n, s.cap, ctx->stage_b.p, ctx->st);
+    CK(cudaGetLastError());
+    std::vector<uint8_t> host(bytes);
+    if (bytes) CK(cudaMemcpyAsync(host.data(), ctx->stage_b.p, bytes, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return write_file(ctx, path, ply ? ply_header(n) : std::string(), host.data(), bytes);
+}
+
+// A parsed PLY -> the planes of `s` (n = its vertex count).
+int load_model(rgs_ctx* ctx, Scene& s, const std::vector<uint8_t>& d, const PlyLayout& L) {
+    if (L.count > (size_t)0x3fffffff) return fail(ctx, RGS_ERR_INVALID_ARG, "too many vertices");
+    if (L.format == 2) {
+        std::vector<float> aos(std::max<size_t>(L.count, 1) * NP);
+        decode_ply_ascii(d, L, aos.data());
+        return upload_gaussians(ctx, s, aos.data(), L.count);
+    }
+    int rc = ensure_scene(ctx, s, (int)L.count, false);
+    if (rc) return rc;
+    s.n = (int)L.count;
+    if (L.count == 0) return RGS_OK;
+    const size_t body = L.count * L.stride;
+    const size_t fbytes = L.fields.size() * sizeof(PlyField);
+    CK(ctx->stage_c.ensure(std::max<size_t>(body, 16)));
+    CK(ctx->stage_d.ensure(std::max<size_t>(fbytes, 16)));
+    if (body) CK(cudaMemcpyAsync(ctx->stage_c.p, d.data() + L.body, body, cudaMemcpyHostToDevice, ctx->st));
+    if (fbytes) CK(cudaMemcpyAsync(ctx->stage_d.p, L.fields.data(), fbytes, cudaMemcpyHostToDevice, ctx->st));
+    launch_unpack_ply(ctx->stage_c.as<uint8_t>(), L.stride, (int)L.count, ctx->stage_d.as<PlyField>(), (int)L.fields.size(),
+                      L.format == 1 ? 1 : 0, s.params.as<float4>(), s.cap, ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->st));  // the host file buffer is released by the caller
+    return RGS_OK;
+}
 
 int check_views(rgs_ctx* ctx, const uint32_t* views, size_t nviews, bool need_targets) {
     if (!views || nviews == 0) return fail(ctx, RGS_ERR_INVALID_ARG, "no views");
@@ -1318,6 +1397,78 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
 }  // namespace
 
 extern "C" {
+
+int rgs_save_ply(rgs_ctx* ctx, const float* gaussians, size_t n, const char* path) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!path || (n && !gaussians)) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
+    if ((rc = upload_gaussians(ctx, ctx->sc, gaussians, n))) return rc;
+    return save_model(ctx, ctx->sc, path, true);
+}
+
+int rgs_save_splat(rgs_ctx* ctx, const float* gaussians, size_t n, const char* path) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!path || (n && !gaussians)) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
+    if ((rc = upload_gaussians(ctx, ctx->sc, gaussians, n))) return rc;
+    return save_model(ctx, ctx->sc, path, false);
+}
+
+int rgs_load_ply(rgs_ctx* ctx, const char* path, float* out, size_t cap, size_t* n_out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!path || !n_out) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
+    std::vector<uint8_t> d;
+    if ((rc = read_file(ctx, path, d))) return rc;
+    PlyLayout L;
+    std::string err;
+    if (parse_ply(d, L, err)) return fail(ctx, RGS_ERR_FORMAT, err + ": " + path);
+    *n_out = L.count;
+    if (!out || cap < L.count) return fail(ctx, RGS_ERR_CAPACITY, "output holds fewer records than the file's vertices");
+    if (L.format == 2) {
+        decode_ply_ascii(d, L, out);
+        return RGS_OK;
+    }
+    Scene& s = ctx->sc;
+    if ((rc = load_model(ctx, s, d, L))) return rc;
+    if (L.count == 0) return RGS_OK;
+    CK(ctx->stage_a.ensure(L.count * NP * sizeof(float)));
+    launch_planes_to_aos(s.params.as<float4>(), ctx->stage_a.as<float>(), s.n, s.cap, ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, ctx->stage_a.p, L.count * NP * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return RGS_OK;
+}
+
+int rgs_trainer_save_ply(rgs_ctx* ctx, const char* path) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!path) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
+    return save_model(ctx, ctx->tr, path, true);
+}
+
+int rgs_trainer_save_splat(rgs_ctx* ctx, const char* path) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!path) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
+    return save_model(ctx, ctx->tr, path, false);
+}
+
+int rgs_trainer_load_ply(rgs_ctx* ctx, const char* path, size_t* n_out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!path) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
+    std::vector<uint8_t> d;
+    if ((rc = read_file(ctx, path, d))) return rc;
+    PlyLayout L;
+    std::string err;
+    if (parse_ply(d, L, err)) return fail(ctx, RGS_ERR_FORMAT, err + ": " + path);
+    Scene& s = ctx->tr;
+    if ((rc = load_model(ctx, s, d, L))) return rc;
+    if ((rc = fresh_adam_state(ctx, s))) return rc;
+    if (n_out) *n_out = L.count;
+    return RGS_OK;
+}
 
 int rgs_trainer_step(rgs_ctx* ctx, const uint32_t* views, size_t nviews, const float bg[3], const rgs_loss_config* loss_cfg,
                      const rgs_train_config* train_cfg, int mode, float* losses_out) {

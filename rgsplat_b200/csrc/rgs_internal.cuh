@@ -24,6 +24,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 namespace rgs {
 
@@ -179,6 +180,27 @@ void launch_blend_store_all(const BlendArgs& a, bool fwd, cudaStream_t st);
 
 // raster.cu: preview framebuffer (colour, 1 - T) as RGBA f32 or sRGB RGBA8.
 void launch_pack_framebuffer(const float* rgb, const float* final_t, size_t npix, int srgb8, void* out, cudaStream_t st);
+
+// ply.cu: io::ply codecs (src/io/ply.rs) on device-resident planes.
+struct PlyField {
+    uint32_t offset;   // byte offset in the vertex record
+    uint8_t width;     // 1, 2, 4 or 8 bytes
+    int16_t target;    // Gaussian3D record index, -1 = skipped
+};
+struct PlyLayout {
+    int format = 2;    // 0 binary LE, 1 binary BE, 2 ascii
+    size_t count = 0;  // vertices
+    size_t stride = 0; // bytes per binary vertex record
+    size_t body = 0;   // byte offset of the body
+    std::vector<PlyField> fields;
+};
+std::string ply_header(size_t n);
+int parse_ply(const std::vector<uint8_t>& data, PlyLayout& layout, std::string& err);
+void decode_ply_ascii(const std::vector<uint8_t>& data, const PlyLayout& layout, float* out /* count * 59 */);
+void launch_pack_ply(const float4* params, int n, int cap, float* out /* n * 62 */, cudaStream_t st);
+void launch_pack_splat(const float4* params, int n, int cap, void* out /* n * 32 bytes */, cudaStream_t st);
+void launch_unpack_ply(const uint8_t* body, size_t stride, int n, const PlyField* fields, int nfields, int big_endian,
+                       float4* params, int cap, cudaStream_t st);
 
 // loss.cu
 void launch_loss(const DevCam* cams, int nviews, int total_blocks, const float* rgb, float lambda,

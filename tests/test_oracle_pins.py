@@ -292,3 +292,54 @@ def test_rasterize_preview_semantics():
     assert np.all(fb[0:16, 0:16] == 0.0) or np.all(fb[32:48, 32:48] == 0.0)
     u8 = O.to_u8_srgb(fb)
     assert u8.dtype == np.uint8 and u8[24, 24, 3] == int(min(max(c[3], 0.0), 1.0) * 255.0)
+
+
+def _ply_roundtrip_scene():
+    from tests import refcases as RC
+
+    g = RC.gaussian_new([1.0, -2.0, 3.5])
+    g[3] = 0.42
+    g[8:11] = [-1.0, -2.0, -0.5]
+    q = np.array([0.3, 0.7, -0.2, 0.5], np.float32)
+    g[4:8] = O.quat_normalize(q)
+    g[11:59] = np.arange(48, dtype=np.float32) * np.float32(0.01) - np.float32(0.2)
+    return np.stack([g, RC.gaussian_new([0.0, 0.0, 0.0])])
+
+
+def test_ply_roundtrip_preserves_parameters():
+    """src/io/ply.rs:290-320 (ply_roundtrip_preserves_parameters)."""
+    orig = _ply_roundtrip_scene()
+    back = O.load_ply_bytes(O.save_ply_bytes(orig))
+    assert back.shape == orig.shape
+    a, b = orig[0], back[0]
+    assert np.all(np.abs(a[0:3] - b[0:3]) < 1e-5) and np.all(np.abs(a[8:11] - b[8:11]) < 1e-5)
+    assert abs(a[3] - b[3]) < 1e-5
+    assert np.all(np.abs(a[11:59] - b[11:59]) < 1e-5)
+    # binary f32 in, f32 out: the round trip is exact
+    assert np.array_equal(orig.view(np.uint32), back.view(np.uint32))
+
+
+def test_splat_record_is_32_bytes():
+    """src/io/ply.rs:322-330 (splat_record_is_32_bytes)."""
+    from tests import refcases as RC
+
+    g = np.stack([RC.gaussian_new([0.0, 0.0, 0.0])] * 10)
+    assert len(O.save_splat_bytes(g)) == 32 * 10
+
+
+def test_ply_reader_formats_and_widths():
+    """load_ply (ply.rs:116-252) reads big-endian and ASCII bodies, any
+    property order, and decodes by byte width alone."""
+    import struct
+
+    props = [("float", "rot_0", 0.5), ("double", "x", 1.25), ("uchar", "opacity", 7), ("ushort", "scale_1", 300),
+             ("float", "f_rest_16", -0.75), ("float", "unknown", 9.0)]
+    head = "ply\nformat {}\nelement vertex 1\n" + "".join(f"property {t} {n}\n" for t, n, _ in props) + "end_header\n"
+    fmt = {"float": "f", "double": "d", "uchar": "B", "ushort": "H"}
+    be = head.format("binary_big_endian 1.0").encode() + b"".join(struct.pack(">" + fmt[t], v) for t, _, v in props)
+    asc = head.format("ascii 1.0").encode() + (" ".join(str(v) for _, _, v in props) + "\n").encode()
+    for data in (be, asc):
+        g = O.load_ply_bytes(data)[0]
+        assert g[4] == 0.5 and g[0] == 1.25 and g[3] == 7.0 and g[9] == 300.0
+        assert g[11 + 16 + 2] == -0.75  # f_rest_16: channel 1, coefficient 2
+        assert g[8] == -3.0 and g[10] == -3.0 and g[5] == 0.0  # Gaussian3D::new defaults
