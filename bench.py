@@ -68,6 +68,7 @@ def parse_args():
     p.add_argument("--ppt", type=int, default=2, help="pixels per thread of the blend kernels (1 or 2)")
     p.add_argument("--no-autotune", action="store_true", help="keep --tile/--batch/--ppt instead of autotuning")
     p.add_argument("--no-variants", action="store_true", help="skip the recompute vs store-all backward measurement")
+    p.add_argument("--no-rows", action="store_true", help="skip the preview / target / model-file row measurements")
     return p.parse_args()
 
 
@@ -194,6 +195,70 @@ def measure_backward_variants(R, scenes, device: int, reps: int = 5) -> dict:
         out[name] = {"forward_ms": round(float(np.median([r["forward_ms"] for r in reps_out])), 4),
                      "backward_ms": round(float(np.median([r["backward_ms"] for r in reps_out])), 4),
                      "blend_state_bytes": int(reps_out[0]["state_bytes"]), "pairs": int(reps_out[0]["pairs"])}
+    return out
+
+
+def measure_next_rows(R, g, cam, device: int, reps: int = 5, cpu: bool = True) -> dict:
+    """The rows either side of the training step, each through its public call
+    with host buffers (host<->device copies and, for the model files, the file
+    write / read inside the time): median of reps after one untimed call, and
+    the oracle on the host cores for the same input (one call each)."""
+    import tempfile
+
+    ctx = R.Context(device=device)
+    rng = np.random.default_rng(9)
+    img = rng.integers(0, 256, size=(cam.height, cam.width, 4), dtype=np.uint8)
+    px = cam.width * cam.height
+    pts = rng.normal(size=(g.shape[0], 3)) * np.array([4.0, 2.0, 3.0])
+    cols = rng.integers(0, 256, size=(g.shape[0], 3), dtype=np.uint8)
+    tmp = tempfile.mkdtemp(prefix="rgs_rows_")
+    ply, splat = os.path.join(tmp, "m.ply"), os.path.join(tmp, "m.splat")
+    n = g.shape[0]
+    rows = {
+        "rasterize_srgb8": (lambda: R.rasterize(g, cam, srgb8=True, ctx=ctx), px * 4,
+                            f"cpu::rasterize + to_u8_srgb, {n} Gaussians, one {cam.width}x{cam.height} view"),
+        "target_srgb8_to_linear": (lambda: R.srgb8_to_linear(img, ctx=ctx), px * 20,
+                                   f"load_target conversion, {cam.width}x{cam.height} RGBA8 -> linear f32"),
+        "save_ply": (lambda: R.save_ply(g, ply, ctx=ctx), n * 248, f"io::ply::save_ply, {n} Gaussians"),
+        "save_splat": (lambda: R.save_splat(g, splat, ctx=ctx), n * 32, f"io::ply::save_splat, {n} Gaussians"),
+        "load_ply": (lambda: R.load_ply(ply, ctx=ctx), n * 248, f"io::ply::load_ply, {n} Gaussians"),
+        "gaussians_from_sfm": (lambda: R.gaussians_from_sfm(pts, cols, ctx=ctx), n * (27 + 236),
+                               f"gaussians_from_sfm + KNN scales, {n} SfM points"),
+    }
+    out = {}
+    for name, (fn, nbytes, what) in rows.items():
+        fn()
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            ts.append(time.perf_counter() - t0)
+        ms = float(np.median(ts)) * 1e3
+        out[name] = {"workload": what, "ms": round(ms, 3), "user_bytes": int(nbytes),
+                     "user_gbs": round(nbytes / (ms / 1e3) / 1e9, 2)}
+    if cpu:
+        import oracle as O
+
+        threads = O.set_threads(os.cpu_count() or 1)
+        ply_bytes = open(ply, "rb").read()
+        oracle_rows = {
+            "rasterize_srgb8": lambda: O.to_u8_srgb(O.rasterize(g, cam)),
+            "target_srgb8_to_linear": lambda: O.srgb8_to_linear(img.reshape(-1, 4)),
+            "save_ply": lambda: open(ply + ".o", "wb").write(O.save_ply_bytes(g)),
+            "save_splat": lambda: open(splat + ".o", "wb").write(O.save_splat_bytes(g)),
+            "load_ply": lambda: O.load_ply_bytes(open(ply, "rb").read()),
+            "gaussians_from_sfm": lambda: O.gaussians_from_sfm(pts, cols),
+        }
+        for name, fn in oracle_rows.items():
+            t0 = time.perf_counter()
+            fn()
+            out[name]["oracle_ms"] = round((time.perf_counter() - t0) * 1e3, 2)
+            out[name]["oracle_threads"] = threads if name == "rasterize_srgb8" else 1
+        del ply_bytes
+    for f in (ply, splat, ply + ".o", splat + ".o"):
+        if os.path.exists(f):
+            os.remove(f)
+    os.rmdir(tmp)
     return out
 
 
@@ -494,6 +559,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         }
         if not args.no_variants:
             line["backward_variants"] = measure_backward_variants(R, scenes, local_rank)
+        if not args.no_rows and world == 1:
+            line["next_rows"] = measure_next_rows(R, g, cfg.cameras[0], local_rank, cpu=not args.no_cpu_baseline)
         # kernels launched per batched step: project 1, depth sort 4x3, count
         # scan 2, emit 1, tile sort 3 per 8 bits, ranges 1, forward 1, loss 2,
         # backward 1, geometry+Adam 2 (+ memsets)

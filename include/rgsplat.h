@@ -237,6 +237,31 @@ int rgs_gpu_render(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_cam
 int rgs_save_ply(rgs_ctx* ctx, const float* gaussians, size_t n, const char* path);
 int rgs_save_splat(rgs_ctx* ctx, const float* gaussians, size_t n, const char* path);
 int rgs_load_ply(rgs_ctx* ctx, const char* path, float* out, size_t cap, size_t* n_out);
+/* gaussians_from_sfm (src/pipeline/sfm.rs:365-404): n SfM points (xyz n*3
+ * f64, rgb n*3 u8) -> n Gaussian3D records (out n*59 f32): the position, the
+ * colour as the SH DC term of powf(u / 255, 2.2), an isotropic log scale of
+ * the mean distance to the 3 nearest points of a 50-wide window of the
+ * x-sorted cloud (estimate_initial_scales, :408-450), identity rotation,
+ * opacity logit(0.1). A non-finite coordinate is RGS_ERR_INVALID_ARG (the
+ * reference's sort panics on NaN). */
+int rgs_gaussians_from_sfm(rgs_ctx* ctx, const double* xyz, const uint8_t* rgb, size_t n, float* out);
+/* The same Gaussians straight into the trainer; the optimiser state restarts. */
+int rgs_trainer_init_from_sfm(rgs_ctx* ctx, const double* xyz, const uint8_t* rgb, size_t n);
+/* parse_points3d_bin (sfm.rs:147-183): a COLMAP points3D.bin on the host.
+ * *n_out = the file's point count; xyz (n*3) and rgb (n*3) are filled when cap
+ * holds them, else RGS_ERR_CAPACITY (call with null buffers to size them).
+ * A file cut short is RGS_ERR_FORMAT. */
+int rgs_read_points3d_bin(rgs_ctx* ctx, const char* path, double* xyz, uint8_t* rgb, size_t cap, size_t* n_out);
+
+/* load_target's colour conversion (src/io/images.rs:67-72, srgb_to_linear
+ * :76-82): 8-bit sRGB RGBA (npix * 4 bytes) -> linear RGBA f32 (npix * 4),
+ * alpha linear. Decoding the file and resizing it to the camera
+ * (image::open, resize_exact) stay with the caller's image library. */
+int rgs_srgb8_to_linear(rgs_ctx* ctx, const uint8_t* rgba8, size_t npix, float* out);
+/* Camera `index`'s target from an 8-bit sRGB RGBA image at the camera's
+ * resolution (w*h*4 bytes), converted to linear on the device. */
+int rgs_trainer_set_target_rgba8(rgs_ctx* ctx, size_t index, const uint8_t* rgba8);
+
 /* The trainer's Gaussians straight from / into device memory; loading resets
  * the Adam state like rgs_trainer_set_gaussians. */
 int rgs_trainer_save_ply(rgs_ctx* ctx, const char* path);

@@ -168,6 +168,13 @@ def _declare(L: C.CDLL) -> None:
     L.orc_rasterize_f.argtypes = [fp, sz, cam, fp, fp]
     L.orc_to_u8_srgb.argtypes = [fp, sz, C.POINTER(C.c_uint8)]
     L.orc_linear_to_srgb.argtypes = [fp, sz, fp]
+    L.orc_srgb8_to_linear.argtypes = [C.POINTER(C.c_uint8), sz, fp]
+    dp = C.POINTER(C.c_double)
+    L.orc_gaussians_from_sfm.argtypes = [dp, C.POINTER(C.c_uint8), sz, fp]
+    L.orc_sfm_scales.argtypes = [dp, sz, fp]
+    L.orc_rust_binary_search.argtypes = [dp, sz, C.c_double, C.POINTER(C.c_int)]
+    L.orc_rust_binary_search.restype = C.c_long
+    L.orc_parse_points3d_bin.argtypes = [C.POINTER(C.c_uint8), sz, dp, C.POINTER(C.c_uint8), sz, C.POINTER(C.c_size_t)]
     u8p = C.POINTER(C.c_uint8)
     L.orc_save_ply.argtypes = [fp, sz, u8p, sz]
     L.orc_save_ply.restype = C.c_long
@@ -340,6 +347,60 @@ def load_ply_bytes(data: bytes) -> np.ndarray:
     out = np.zeros((n.value, 59), np.float32)
     _check(lib().orc_load_ply(p, buf.size, _f(out), n.value, C.byref(n)), "load_ply")
     return out
+
+
+def srgb8_to_linear(rgba8) -> np.ndarray:
+    """``load_target``'s conversion (src/io/images.rs:67-72): RGBA8 -> linear RGBA f32."""
+    a = np.ascontiguousarray(rgba8, np.uint8)
+    out = np.zeros(a.shape, np.float32)
+    _check(lib().orc_srgb8_to_linear(a.ctypes.data_as(C.POINTER(C.c_uint8)), a.size // 4, _f(out)), "srgb8_to_linear")
+    return out
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def gaussians_from_sfm(xyz, rgb) -> np.ndarray:
+    """``gaussians_from_sfm`` (src/pipeline/sfm.rs:365-404): (N, 3) f64 points and
+    (N, 3) u8 colours -> (N, 59) Gaussians."""
+    x = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)
+    c = np.ascontiguousarray(rgb, np.uint8).reshape(-1, 3)
+    if x.shape[0] != c.shape[0]:
+        raise ValueError("xyz and rgb hold different point counts")
+    out = np.zeros((x.shape[0], 59), np.float32)
+    _check(lib().orc_gaussians_from_sfm(_dp(x), c.ctypes.data_as(C.POINTER(C.c_uint8)), x.shape[0], _f(out)),
+           "gaussians_from_sfm")
+    return out
+
+
+def sfm_scales(xyz) -> np.ndarray:
+    """``estimate_initial_scales`` (src/pipeline/sfm.rs:408-450) -> (N,) f32."""
+    x = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)
+    out = np.zeros(x.shape[0], np.float32)
+    _check(lib().orc_sfm_scales(_dp(x), x.shape[0], _f(out)), "sfm_scales")
+    return out
+
+
+def rust_binary_search(xs, t: float):
+    """Rust's slice::binary_search_by on sorted f64 keys -> ("ok" | "err", index)."""
+    a = np.ascontiguousarray(xs, np.float64)
+    ok = C.c_int(0)
+    r = lib().orc_rust_binary_search(_dp(a), a.size, float(t), C.byref(ok))
+    return ("ok" if ok.value else "err", int(r))
+
+
+def parse_points3d_bin(data: bytes):
+    """``parse_points3d_bin`` (src/pipeline/sfm.rs:147-183) -> (xyz (N, 3) f64, rgb (N, 3) u8)."""
+    buf = np.frombuffer(data, np.uint8)
+    p = buf.ctypes.data_as(C.POINTER(C.c_uint8))
+    n = C.c_size_t(0)
+    _check(lib().orc_parse_points3d_bin(p, buf.size, None, None, 0, C.byref(n)), "parse_points3d_bin")
+    xyz = np.zeros((n.value, 3), np.float64)
+    rgb = np.zeros((n.value, 3), np.uint8)
+    _check(lib().orc_parse_points3d_bin(p, buf.size, _dp(xyz), rgb.ctypes.data_as(C.POINTER(C.c_uint8)), n.value,
+                                        C.byref(n)), "parse_points3d_bin")
+    return xyz, rgb
 
 
 def to_u8_srgb(rgba) -> np.ndarray:

@@ -7,6 +7,7 @@
 
 #include "oracle.hpp"
 #include "ply.hpp"
+#include "sfm.hpp"
 
 namespace orc {
 int g_libm_math = 0;
@@ -66,6 +67,47 @@ int orc_rasterize_f(const float* g, size_t n, const orc_camera* cam, const float
 
 int orc_linear_to_srgb(const float* x, size_t n, float* out) {
     for (size_t i = 0; i < n; ++i) out[i] = fm::linear_to_srgb(x[i]);
+    return ORC_OK;
+}
+
+// images.rs:67-72: RGBA8 -> linear RGBA f32 (alpha linear)
+// sfm.rs:365-450
+int orc_gaussians_from_sfm(const double* xyz, const uint8_t* rgb, size_t n, float* out) {
+    if (n && (!xyz || !rgb || !out)) return ORC_EINVAL;
+    for (size_t i = 0; i < 3 * n; ++i)
+        if (!std::isfinite(xyz[i])) return ORC_EINVAL;
+    sfm::gaussians_from_sfm(xyz, rgb, n, out);
+    return ORC_OK;
+}
+int orc_sfm_scales(const double* xyz, size_t n, float* out) {
+    if (n && (!xyz || !out)) return ORC_EINVAL;
+    sfm::estimate_initial_scales(xyz, n, out);
+    return ORC_OK;
+}
+long orc_rust_binary_search(const double* xs, size_t n, double t, int* ok) {
+    bool b = false;
+    const size_t r = sfm::rust_binary_search(xs, n, t, &b);
+    *ok = b ? 1 : 0;
+    return (long)r;
+}
+// sfm.rs:147-183; *n_out = point count, records copied when cap holds them
+int orc_parse_points3d_bin(const uint8_t* data, size_t size, double* xyz, uint8_t* rgb, size_t cap, size_t* n_out) {
+    std::vector<sfm::Point> pts;
+    if (sfm::parse_points3d_bin(data, size, pts)) return ORC_EINVAL;
+    *n_out = pts.size();
+    if (xyz && rgb && cap >= pts.size())
+        for (size_t i = 0; i < pts.size(); ++i) {
+            std::memcpy(xyz + 3 * i, pts[i].xyz, 24);
+            std::memcpy(rgb + 3 * i, pts[i].rgb, 3);
+        }
+    return ORC_OK;
+}
+
+int orc_srgb8_to_linear(const uint8_t* rgba8, size_t npix, float* out) {
+    for (size_t i = 0; i < npix * 4; ++i) {
+        const float x = (float)rgba8[i] / 255.0f;
+        out[i] = i % 4 == 3 ? x : fm::srgb_to_linear(x);
+    }
     return ORC_OK;
 }
 

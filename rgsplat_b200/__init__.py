@@ -19,6 +19,10 @@ from .api import (  # noqa: F401
     estimate_scene_extent,
     photometric_loss_grad,
     rasterize,
+    black_target,
+    srgb8_to_linear,
+    gaussians_from_sfm,
+    read_points3d_bin,
     load_ply,
     save_ply,
     save_splat,

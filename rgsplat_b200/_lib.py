@@ -174,6 +174,11 @@ SIGNATURES = {
     "rgs_save_ply": (C.c_int, [CTX, FP, C.c_size_t, C.c_char_p]),
     "rgs_save_splat": (C.c_int, [CTX, FP, C.c_size_t, C.c_char_p]),
     "rgs_load_ply": (C.c_int, [CTX, C.c_char_p, FP, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "rgs_gaussians_from_sfm": (C.c_int, [CTX, C.c_void_p, C.c_void_p, C.c_size_t, FP]),
+    "rgs_trainer_init_from_sfm": (C.c_int, [CTX, C.c_void_p, C.c_void_p, C.c_size_t]),
+    "rgs_read_points3d_bin": (C.c_int, [CTX, C.c_char_p, C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "rgs_srgb8_to_linear": (C.c_int, [CTX, C.c_void_p, C.c_size_t, FP]),
+    "rgs_trainer_set_target_rgba8": (C.c_int, [CTX, C.c_size_t, C.c_void_p]),
     "rgs_trainer_save_ply": (C.c_int, [CTX, C.c_char_p]),
     "rgs_trainer_save_splat": (C.c_int, [CTX, C.c_char_p]),
     "rgs_trainer_load_ply": (C.c_int, [CTX, C.c_char_p, C.POINTER(C.c_size_t)]),

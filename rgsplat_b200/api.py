@@ -305,6 +305,25 @@ def rasterize(gaussians, camera: Camera, bg=(0.0, 0.0, 0.0), srgb8: bool = False
     return out
 
 
+def srgb8_to_linear(rgba8, ctx: Context | None = None) -> np.ndarray:
+    """``load_target``'s conversion (src/io/images.rs:67-72): an 8-bit sRGB RGBA
+    image (..., 4) uint8 -> linear RGBA float32 of the same shape."""
+    ctx = ctx or default_context()
+    a = np.ascontiguousarray(rgba8, np.uint8)
+    if a.size % 4:
+        raise ValueError("RGBA8 input must hold 4 bytes per pixel")
+    out = np.zeros(a.shape, np.float32)
+    ctx.check(ctx.lib.rgs_srgb8_to_linear(ctx.handle, a.ctypes.data, a.size // 4, _fp(out)))
+    return out
+
+
+def black_target(width: int, height: int) -> np.ndarray:
+    """``TargetImage::black`` (src/io/images.rs:26-33): opaque black RGBA (h, w, 4)."""
+    t = np.zeros((height, width, 4), np.float32)
+    t[..., 3] = 1.0
+    return t
+
+
 def save_ply(gaussians, path, ctx: Context | None = None) -> None:
     """``io::ply::save_ply`` (src/io/ply.rs:35-104): binary little-endian 3DGS .ply."""
     ctx = ctx or default_context()
@@ -330,6 +349,40 @@ def load_ply(path, ctx: Context | None = None) -> np.ndarray:
     out = np.zeros((max(n.value, 1), GAUSSIAN_FLOATS), np.float32)
     ctx.check(ctx.lib.rgs_load_ply(ctx.handle, p, _fp(out), out.shape[0], C.byref(n)))
     return out[: n.value]
+
+
+def _sfm_points(xyz, rgb):
+    x = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)
+    c = np.ascontiguousarray(rgb, np.uint8).reshape(-1, 3)
+    if x.shape[0] != c.shape[0]:
+        raise ValueError("xyz and rgb hold different point counts")
+    return x, c
+
+
+def gaussians_from_sfm(xyz, rgb, ctx: Context | None = None) -> np.ndarray:
+    """``gaussians_from_sfm`` (src/pipeline/sfm.rs:365-404) on the device: (N, 3)
+    f64 points and (N, 3) u8 colours -> (N, 59) Gaussians, scales from
+    ``estimate_initial_scales`` (:408-450)."""
+    ctx = ctx or default_context()
+    x, c = _sfm_points(xyz, rgb)
+    out = np.zeros((x.shape[0], GAUSSIAN_FLOATS), np.float32)
+    ctx.check(ctx.lib.rgs_gaussians_from_sfm(ctx.handle, x.ctypes.data, c.ctypes.data, x.shape[0], _fp(out)))
+    return out
+
+
+def read_points3d_bin(path, ctx: Context | None = None):
+    """``parse_points3d_bin`` (src/pipeline/sfm.rs:147-183) of a COLMAP
+    points3D.bin -> (xyz (N, 3) f64, rgb (N, 3) u8)."""
+    ctx = ctx or default_context()
+    n = C.c_size_t(0)
+    p = os.fsencode(path)
+    rc = ctx.lib.rgs_read_points3d_bin(ctx.handle, p, None, None, 0, C.byref(n))
+    if rc not in (L.RGS_OK, L.RGS_ERR_CAPACITY):
+        ctx.check(rc)
+    xyz = np.zeros((max(n.value, 1), 3), np.float64)
+    rgb = np.zeros((max(n.value, 1), 3), np.uint8)
+    ctx.check(ctx.lib.rgs_read_points3d_bin(ctx.handle, p, xyz.ctypes.data, rgb.ctypes.data, xyz.shape[0], C.byref(n)))
+    return xyz[: n.value], rgb[: n.value]
 
 
 def photometric_loss_grad(rendered, target_rgba, w: int, h: int, lam: float, ctx: Context | None = None):
@@ -484,6 +537,22 @@ class Trainer:
         self.ctx.check(self.lib.rgs_trainer_step(self.ctx.handle, v.ctypes.data_as(L.U32P), v.size, _fp(_f32(bg)), C.byref(lc),
                                                  C.byref(tc), int(mode), _fp(losses)))
         return losses[: v.size]
+
+    def init_from_sfm(self, xyz, rgb) -> int:
+        """The trainer's Gaussians from SfM points (``gaussians_from_sfm``,
+        src/pipeline/sfm.rs:365-450) built on the device; the optimiser restarts."""
+        x, c = _sfm_points(xyz, rgb)
+        self.ctx.check(self.lib.rgs_trainer_init_from_sfm(self.ctx.handle, x.ctypes.data, c.ctypes.data, x.shape[0]))
+        return x.shape[0]
+
+    def set_target_rgba8(self, index: int, rgba8) -> None:
+        """Camera ``index``'s target from an 8-bit sRGB RGBA image at the camera's
+        resolution, converted to linear on the device (images.rs:67-72)."""
+        a = np.ascontiguousarray(rgba8, np.uint8)
+        c = self.cameras[index]
+        if a.size != c.width * c.height * 4:
+            raise ValueError("target must be h*w*4 bytes")
+        self.ctx.check(self.lib.rgs_trainer_set_target_rgba8(self.ctx.handle, int(index), a.ctypes.data))
 
     def save_ply(self, path) -> None:
         """The device-resident Gaussians as a 3DGS .ply (io::ply::save_ply)."""

@@ -81,6 +81,7 @@ struct rgs_ctx {
     DBuf ranges, rgb, final_t, last, dl, partials;
     DBuf scalars, block_sums;
     SortScratch sort;
+    SfmScratch sfm;
     DBuf dens_scratch, dens_out, m_tmp;
     DBuf stage_a, stage_b, stage_c, stage_d, target_stage;
     DBuf tstore;  // store-all backward study only
@@ -675,6 +676,7 @@ void rgs_destroy(rgs_ctx* ctx) {
                     &ctx->dens_out, &ctx->m_tmp, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->stage_d,
                     &ctx->target_stage, &ctx->tstore};
     for (DBuf* b : bufs) b->release();
+    ctx->sfm.release();
     if (ctx->hdr_h) cudaFreeHost(ctx->hdr_h);
     if (ctx->out_h) cudaFreeHost(ctx->out_h);
     for (int i = 0; i <= RGS_NUM_STAGES; ++i)
@@ -1175,6 +1177,57 @@ int load_model(rgs_ctx* ctx, Scene& s, const std::vector<uint8_t>& d, const PlyL
     return RGS_OK;
 }
 
+// gaussians_from_sfm into s.params (s.n = n).
+int sfm_to_scene(rgs_ctx* ctx, Scene& s, const double* xyz, const uint8_t* rgb, size_t n) {
+    if (n > (size_t)0x3fffffff) return fail(ctx, RGS_ERR_INVALID_ARG, "too many points");
+    int rc = ensure_scene(ctx, s, (int)n, false);
+    if (rc) return rc;
+    s.n = (int)n;
+    if (n == 0) return RGS_OK;
+    SfmScratch& w = ctx->sfm;
+    CK(w.xyz.ensure(n * 24));
+    CK(w.rgb.ensure(n * 3 + 16));
+    CK(cudaMemcpyAsync(w.xyz.p, xyz, n * 24, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(w.rgb.p, rgb, n * 3, cudaMemcpyHostToDevice, ctx->st));
+    int bad = 0;
+    cudaError_t e = cudaSuccess;
+    sfm_init_planes(w.xyz.as<double>(), w.rgb.as<uint8_t>(), (int)n, s.params.as<float4>(), s.cap, w, sort_grid_blocks(),
+                    ctx->st, &bad, &e);
+    CK(e);
+    if (bad) {
+        s.n = 0;
+        return fail(ctx, RGS_ERR_INVALID_ARG, "non-finite SfM point coordinate");
+    }
+    return RGS_OK;
+}
+
+// parse_points3d_bin (sfm.rs:147-183) over a file's bytes.
+int parse_points3d(rgs_ctx* ctx, const std::vector<uint8_t>& d, std::vector<double>& xyz, std::vector<uint8_t>& rgb) {
+    size_t at = 0;
+    auto take = [&](void* dst, size_t k) {
+        if (d.size() - at < k) return false;
+        std::memcpy(dst, d.data() + at, k);
+        at += k;
+        return true;
+    };
+    uint64_t count = 0;
+    if (!take(&count, 8)) return fail(ctx, RGS_ERR_FORMAT, "points3D.bin: no point count");
+    xyz.clear();
+    rgb.clear();
+    for (uint64_t r = 0; r < count; ++r) {
+        uint64_t id = 0, track = 0;
+        double p[3], err = 0.0;
+        uint8_t c[3];
+        if (!take(&id, 8) || !take(p, 24) || !take(c, 3) || !take(&err, 8) || !take(&track, 8))
+            return fail(ctx, RGS_ERR_FORMAT, "points3D.bin: record cut short");
+        if (track > (d.size() - at) / 8) return fail(ctx, RGS_ERR_FORMAT, "points3D.bin: track cut short");
+        at += (size_t)track * 8;
+        xyz.insert(xyz.end(), p, p + 3);
+        rgb.insert(rgb.end(), c, c + 3);
+    }
+    return RGS_OK;
+}
+
 int check_views(rgs_ctx* ctx, const uint32_t* views, size_t nviews, bool need_targets) {
     if (!views || nviews == 0) return fail(ctx, RGS_ERR_INVALID_ARG, "no views");
     if (nviews > (size_t)MAX_VIEWS) return fail(ctx, RGS_ERR_INVALID_ARG, "at most 64 views per step");
@@ -1436,6 +1489,78 @@ int rgs_load_ply(rgs_ctx* ctx, const char* path, float* out, size_t cap, size_t*
     launch_planes_to_aos(s.params.as<float4>(), ctx->stage_a.as<float>(), s.n, s.cap, ctx->st);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, ctx->stage_a.p, L.count * NP * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return RGS_OK;
+}
+
+int rgs_gaussians_from_sfm(rgs_ctx* ctx, const double* xyz, const uint8_t* rgb, size_t n, float* out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (n && (!xyz || !rgb || !out)) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
+    Scene& s = ctx->sc;
+    if ((rc = sfm_to_scene(ctx, s, xyz, rgb, n))) return rc;
+    if (n == 0) return RGS_OK;
+    CK(ctx->stage_a.ensure(n * NP * sizeof(float)));
+    launch_planes_to_aos(s.params.as<float4>(), ctx->stage_a.as<float>(), s.n, s.cap, ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, ctx->stage_a.p, n * NP * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return RGS_OK;
+}
+
+int rgs_trainer_init_from_sfm(rgs_ctx* ctx, const double* xyz, const uint8_t* rgb, size_t n) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (n && (!xyz || !rgb)) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
+    Scene& s = ctx->tr;
+    if ((rc = sfm_to_scene(ctx, s, xyz, rgb, n))) return rc;
+    return fresh_adam_state(ctx, s);
+}
+
+int rgs_read_points3d_bin(rgs_ctx* ctx, const char* path, double* xyz, uint8_t* rgb, size_t cap, size_t* n_out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!path || !n_out) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
+    std::vector<uint8_t> d;
+    if ((rc = read_file(ctx, path, d))) return rc;
+    std::vector<double> px;
+    std::vector<uint8_t> pc;
+    if ((rc = parse_points3d(ctx, d, px, pc))) return rc;
+    const size_t n = pc.size() / 3;
+    *n_out = n;
+    if (!xyz || !rgb || cap < n) return fail(ctx, RGS_ERR_CAPACITY, "output holds fewer points than the file");
+    if (n) {
+        std::memcpy(xyz, px.data(), n * 24);
+        std::memcpy(rgb, pc.data(), n * 3);
+    }
+    return RGS_OK;
+}
+
+int rgs_srgb8_to_linear(rgs_ctx* ctx, const uint8_t* rgba8, size_t npix, float* out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (npix && (!rgba8 || !out)) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
+    if (npix == 0) return RGS_OK;
+    CK(ctx->stage_a.ensure(npix * 4));
+    CK(ctx->stage_b.ensure(npix * 16));
+    CK(cudaMemcpyAsync(ctx->stage_a.p, rgba8, npix * 4, cudaMemcpyHostToDevice, ctx->st));
+    launch_srgb8_to_linear(ctx->stage_a.p, npix, ctx->stage_b.as<float>(), ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, ctx->stage_b.p, npix * 16, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return RGS_OK;
+}
+
+int rgs_trainer_set_target_rgba8(rgs_ctx* ctx, size_t index, const uint8_t* rgba8) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (index >= ctx->cams.size() || !rgba8) return fail(ctx, RGS_ERR_INVALID_ARG, "bad camera index or null target");
+    const size_t px = (size_t)ctx->cams[index].width * ctx->cams[index].height;
+    CK(ctx->targets[index].ensure(px * 16));
+    CK(ctx->stage_a.ensure(std::max<size_t>(px * 4, 16)));
+    CK(cudaMemcpyAsync(ctx->stage_a.p, rgba8, px * 4, cudaMemcpyHostToDevice, ctx->st));
+    launch_srgb8_to_linear(ctx->stage_a.p, px, ctx->targets[index].as<float>(), ctx->st);
+    CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->st));
     return RGS_OK;
 }

@@ -1,8 +1,12 @@
-// raster.cu -- cpu::rasterize's output stage (src/cpu/rasterizer.rs:38-48,
-// 171-186): the preview framebuffer as RGBA float (colour, 1 - T) or as
-// Framebuffer::to_u8_srgb's gamma-encoded RGBA8, packed on the device from
-// the forward blend's colour and final transmittance so only the final
-// format crosses to the host.
+// raster.cu -- colour-space conversions at the two ends of the path:
+//   * cpu::rasterize's output stage (src/cpu/rasterizer.rs:38-48, 171-186):
+//     the preview framebuffer as RGBA float (colour, 1 - T) or as
+//     Framebuffer::to_u8_srgb's gamma-encoded RGBA8, packed on the device
+//     from the forward blend's colour and final transmittance so only the
+//     final format crosses to the host;
+//   * load_target's input stage (src/io/images.rs:67-72): an 8-bit sRGB
+//     RGBA image becomes the loss's linear RGBA f32 target on the device, so
+//     4 bytes per pixel cross PCIe instead of 16.
 #include "rgs_internal.cuh"
 #include "rgs_math.cuh"
 
@@ -23,6 +27,25 @@ __global__ void __launch_bounds__(256) k_pack_srgb8(const float* __restrict__ rg
     for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += (size_t)gridDim.x * blockDim.x)
         out[p] = make_uchar4(srgb8(rgb[p * 3]), srgb8(rgb[p * 3 + 1]), srgb8(rgb[p * 3 + 2]),
                              as_u8(rclamp(1.0f - final_t[p], 0.0f, 1.0f) * 255.0f));
+}
+
+// One thread per pixel: RGB through srgb_to_linear(u / 255), alpha u / 255.
+__global__ void __launch_bounds__(256) k_srgb8_to_linear(const uchar4* __restrict__ in, size_t npix, float4* __restrict__ out) {
+    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += (size_t)gridDim.x * blockDim.x) {
+        const uchar4 c = in[p];
+        out[p] = make_float4(srgb_to_linear((float)c.x / 255.0f), srgb_to_linear((float)c.y / 255.0f),
+                             srgb_to_linear((float)c.z / 255.0f), (float)c.w / 255.0f);
+    }
+}
+
+void launch_srgb8_to_linear(const void* rgba8, size_t npix, float* out, cudaStream_t st) {
+    if (npix == 0) return;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t want = (npix + 255) / 256;
+    const unsigned grid = (unsigned)(want < (size_t)sms * 8 ? want : (size_t)sms * 8);
+    k_srgb8_to_linear<<<grid, 256, 0, st>>>((const uchar4*)rgba8, npix, (float4*)out);
 }
 
 void launch_pack_framebuffer(const float* rgb, const float* final_t, size_t npix, int srgb8, void* out, cudaStream_t st) {

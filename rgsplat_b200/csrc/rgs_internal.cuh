@@ -105,6 +105,17 @@ struct SortScratch {
     DBuf keys2, vals2;
 };
 
+// Device scratch of the SfM initialisation (sfm.cu): its own sort buffers, so
+// the trainer's captured step never sees them change.
+struct SfmScratch {
+    DBuf xyz, rgb;           // the points as uploaded
+    DBuf u32, f64, scales, flag;
+    SortScratch sort;
+    void release() {
+        for (DBuf* b : {&xyz, &rgb, &u32, &f64, &scales, &flag, &sort.hist, &sort.keys2, &sort.vals2}) b->release();
+    }
+};
+
 // ---- launchers (each defined in the .cu file named in the comment) --------
 
 // layout.cu
@@ -180,6 +191,13 @@ void launch_blend_store_all(const BlendArgs& a, bool fwd, cudaStream_t st);
 
 // raster.cu: preview framebuffer (colour, 1 - T) as RGBA f32 or sRGB RGBA8.
 void launch_pack_framebuffer(const float* rgb, const float* final_t, size_t npix, int srgb8, void* out, cudaStream_t st);
+// sfm.cu: gaussians_from_sfm (sfm.rs:365-450) from device-resident points
+// (xyz n*3 f64, rgb n*3 u8) into parameter planes [NPL][cap]. *bad_host is set
+// when a coordinate is not finite (the planes then hold no defined values).
+int sfm_init_planes(const double* xyz, const uint8_t* rgb, int n, float4* planes, int cap, SfmScratch& w, int grid,
+                    cudaStream_t st, int* bad_host, cudaError_t* err);
+// 8-bit sRGB RGBA -> linear RGBA f32 (images.rs:67-72).
+void launch_srgb8_to_linear(const void* rgba8, size_t npix, float* out, cudaStream_t st);
 
 // ply.cu: io::ply codecs (src/io/ply.rs) on device-resident planes.
 struct PlyField {

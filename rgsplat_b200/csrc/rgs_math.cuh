@@ -99,6 +99,14 @@ __device__ __forceinline__ float linear_to_srgb(float x) {
     return 1.055f * p - 0.055f;
 }
 
+// srgb_to_linear (src/io/images.rs:76-82): ((x + 0.055) / 1.055).powf(2.4)
+// evaluated as exp(2.4 ln t) in double and rounded once.
+__device__ __forceinline__ float srgb_to_linear(float x) {
+    if (x <= 0.04045f) return x / 12.92f;
+    const float t = (x + 0.055f) / 1.055f;
+    return __double2float_rn(exp_core_d(2.4 * log_pos_d((double)t)));
+}
+
 // Rust `f as u8`: truncate toward zero, saturate, NaN -> 0.
 __device__ __forceinline__ unsigned char as_u8(float f) {
     if (!(f > 0.0f)) return 0;

@@ -76,3 +76,81 @@ def loss_grad_images(w=12, h=12):
 
 # Gradient record (GaussianGrad, src/cpu/backward.rs:33-41)
 G_POS, G_ROT, G_SCL, G_OPA, G_SH, G_SCREEN = slice(0, 3), slice(3, 7), slice(7, 10), 10, slice(11, 59), 59
+
+
+# ---------------------------------------------------------------------------
+# estimate_initial_scales (src/pipeline/sfm.rs:408-450) in plain Python, a
+# second restatement for pinning the C oracle on small clouds.
+# ---------------------------------------------------------------------------
+def rust_binary_search_py(xs, t):
+    """Rust's slice::binary_search_by, size-halving form (last of equal keys)."""
+    n = len(xs)
+    if n == 0:
+        return ("err", 0)
+    base, size = 0, n
+    while size > 1:
+        half = size // 2
+        mid = base + half
+        if not xs[mid] > t:
+            base = mid
+        size -= half
+    if xs[base] == t:
+        return ("ok", base)
+    return ("err", base + (1 if xs[base] < t else 0))
+
+
+def sfm_scales_py(xyz):
+    import math
+
+    pts = [tuple(float(v) for v in p) for p in xyz]
+    n = len(pts)
+    order = sorted(range(n), key=lambda i: pts[i][0])  # stable
+    sx = [pts[i][0] for i in order]
+    out = []
+    window = min(50, n)
+    for i, q in enumerate(pts):
+        kind, found = rust_binary_search_py(sx, q[0])
+        if kind != "ok":
+            found = 0
+        start = found - min(found, window // 2)
+        end = min(start + window, n)
+        d = []
+        for p in range(start, end):
+            j = order[p]
+            if j == i:
+                continue
+            o = pts[j]
+            dx, dy, dz = o[0] - q[0], o[1] - q[1], o[2] - q[2]
+            d.append(math.sqrt(dx * dx + dy * dy + dz * dz))
+        d.sort()
+        if not d:
+            out.append(0.01)
+        else:
+            k = min(3, len(d))
+            s = -0.0
+            for v in d[:k]:
+                s += v
+            out.append(s / k)
+    import numpy as np
+
+    return np.array(out, dtype=np.float64).astype(np.float32)
+
+
+def sfm_cloud(n, seed, dup_x=0):
+    """A seeded SfM-like cloud: clustered points, some exactly repeated, some
+    sharing x, a -0.0 / +0.0 pair, colours over the full byte range."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    c = rng.normal(size=(max(n // 40, 1), 3)) * 3.0
+    xyz = c[rng.integers(0, c.shape[0], n)] + rng.normal(size=(n, 3)) * 0.05
+    if n >= 8:
+        xyz[1] = xyz[0]                      # an exact duplicate point
+        xyz[3, 0] = xyz[2, 0]                # same x, different y / z
+        xyz[4, 0], xyz[5, 0] = -0.0, 0.0     # signed zeros compare equal
+    if dup_x:
+        xyz[-dup_x:, 0] = xyz[-1, 0]         # a long run of equal x
+    rgb = rng.integers(0, 256, size=(n, 3), dtype=np.uint8)
+    if n >= 2:
+        rgb[0] = (0, 255, 128)
+    return xyz, rgb

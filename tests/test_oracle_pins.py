@@ -12,6 +12,7 @@ import pytest
 
 import oracle as O
 from tests import refcases as R
+from tests import refcases as RC
 
 
 # ---- src/math/mod.rs:215-231 ------------------------------------------------
@@ -270,6 +271,44 @@ def test_linear_srgb():
     assert v[2] > 0.5
 
 
+def test_srgb_linear_endpoints():
+    """src/io/images.rs:88-94 (srgb_linear_endpoints), through load_target's
+    byte path (images.rs:64-70): 0 -> 0, 255 -> 1, mid-tones darker."""
+    lin = O.srgb8_to_linear(np.array([[0, 255, 128, 0]], np.uint8))
+    assert abs(lin[0, 0]) < 1e-6
+    assert abs(lin[0, 1] - 1.0) < 1e-5
+    assert lin[0, 2] < 128 / 255
+    assert lin[0, 3] == 0.0
+
+
+def test_srgb8_to_linear_every_byte():
+    """images.rs:64-82 for all 256 byte values: the linear branch is x / 12.92,
+    the power branch is powf(t, 2.4) with t = (x + 0.055) / 1.055 in f32,
+    alpha is u / 255; the oracle's exp(2.4 ln t) in double rounds to the same
+    f32 as a float64 pow for every byte, and linear_to_srgb inverts it."""
+    u = np.arange(256, dtype=np.uint8)
+    img = np.stack([u, u, u, u], 1)
+    lin = O.srgb8_to_linear(img)
+    x = u.astype(np.float32) / np.float32(255.0)
+    t = (x + np.float32(0.055)) / np.float32(1.055)
+    want = np.where(x <= np.float32(0.04045), x / np.float32(12.92),
+                    (t.astype(np.float64) ** 2.4).astype(np.float32)).astype(np.float32)
+    assert np.array_equal(lin[:, 0].view(np.uint32), want.view(np.uint32))
+    assert np.array_equal(lin[:, 3].view(np.uint32), x.view(np.uint32))
+    assert np.all(np.diff(lin[:, 0]) > 0)
+    back = O.linear_to_srgb(lin[:, 0])
+    assert np.max(np.abs(back - x)) < 2e-6
+
+
+def test_black_target_has_opaque_alpha():
+    """images.rs:96-101 (black_image_has_opaque_alpha): TargetImage::black."""
+    import rgsplat_b200 as R
+
+    img = R.black_target(4, 4)
+    assert img.size == 4 * 4 * 4
+    assert img.reshape(-1)[3] == 1.0 and np.all(img[..., :3] == 0.0)
+
+
 def test_rasterize_preview_semantics():
     """rasterizer.rs:72-192: colour starts at bg (not bg * T), alpha = 1 - T,
     tiles no splat touches stay (0, 0, 0, 0)."""
@@ -343,3 +382,86 @@ def test_ply_reader_formats_and_widths():
         assert g[4] == 0.5 and g[0] == 1.25 and g[3] == 7.0 and g[9] == 300.0
         assert g[11 + 16 + 2] == -0.75  # f_rest_16: channel 1, coefficient 2
         assert g[8] == -3.0 and g[10] == -3.0 and g[5] == 0.0  # Gaussian3D::new defaults
+
+
+# ---------------------------------------------------------------------------
+# SfM initialisation (src/pipeline/sfm.rs:142-183, 365-450). The reference has
+# no tests or fixtures for it and no Rust toolchain is available here, so the
+# C oracle is pinned against a second, plain-Python restatement and against
+# the closed forms of each field.
+# ---------------------------------------------------------------------------
+def test_rust_binary_search_matches_restatement():
+    rng = np.random.default_rng(5)
+    for n in (0, 1, 2, 7, 64, 257):
+        xs = np.sort(rng.integers(0, 12, n).astype(np.float64))
+        for t in list(xs) + [-1.0, 5.5, 20.0]:
+            assert O.rust_binary_search(xs, t) == RC.rust_binary_search_py(list(xs), t)
+    # among equal keys the size-halving search lands on the last one
+    assert O.rust_binary_search([1.0, 2.0, 2.0, 2.0, 3.0], 2.0) == ("ok", 3)
+
+
+@pytest.mark.parametrize("n,seed,dup", [(1, 1, 0), (2, 2, 0), (3, 3, 0), (49, 4, 0), (50, 5, 0), (51, 6, 0),
+                                        (300, 7, 0), (400, 8, 60), (257, 9, 30)])
+def test_sfm_scales_match_python_restatement(n, seed, dup):
+    xyz, _ = RC.sfm_cloud(n, seed, dup)
+    assert np.array_equal(O.sfm_scales(xyz).view(np.uint32), RC.sfm_scales_py(xyz).view(np.uint32))
+
+
+def test_gaussians_from_sfm_fields():
+    xyz, rgb = RC.sfm_cloud(300, 11)
+    u = np.arange(256, dtype=np.uint8)
+    rgb[:256] = np.stack([u, u[::-1], np.roll(u, 7)], 1)
+    g = O.gaussians_from_sfm(xyz, rgb)
+    assert g.shape == (300, 59)
+    assert np.array_equal(g[:, 0:3], xyz.astype(np.float32))
+    # math::logit(0.1) and Gaussian3D::new's identity rotation
+    p = np.float32(0.1)
+    assert np.all(g[:, 3] == np.float32(np.log(np.float64(p / (np.float32(1) - p)))))
+    assert np.all(g[:, 4:8] == np.array([1, 0, 0, 0], np.float32))
+    # isotropic log scale of the clamped KNN scale
+    s = np.maximum(O.sfm_scales(xyz), np.float32(1e-4))
+    ls = np.log(s.astype(np.float64)).astype(np.float32)
+    assert np.all(g[:, 8] == ls) and np.all(g[:, 9] == ls) and np.all(g[:, 10] == ls)
+    # DC terms (sh 0, 16, 32): (powf(u / 255, 2.2) - 0.5) * (1 / SH_C0), the
+    # power rounding like a float64 pow for every byte value
+    inv = np.float32(1.0) / np.float32(0.28209479177387814)
+    for c in range(3):
+        x = rgb[:, c].astype(np.float32) / np.float32(255.0)
+        lin = np.where(x == 0, np.float32(0), (x.astype(np.float64) ** np.float64(np.float32(2.2))).astype(np.float32))
+        want = (lin.astype(np.float32) - np.float32(0.5)) * inv
+        assert np.array_equal(g[:, 11 + 16 * c].view(np.uint32), want.astype(np.float32).view(np.uint32))
+    rest = np.delete(g[:, 11:], [0, 16, 32], axis=1)
+    assert np.all(rest == 0.0)
+
+
+def test_gaussians_from_sfm_edges():
+    assert O.gaussians_from_sfm(np.zeros((0, 3)), np.zeros((0, 3), np.uint8)).shape == (0, 59)
+    one = O.gaussians_from_sfm([[1.0, 2.0, 3.0]], [[10, 20, 30]])
+    assert one[0, 8] == np.float32(np.log(np.float64(np.float32(0.01))))  # no neighbour: 0.01
+    # coincident points: distance 0 -> scale clamped to 1e-4
+    two = O.gaussians_from_sfm([[1.0, 2.0, 3.0], [1.0, 2.0, 3.0]], [[0, 0, 0], [255, 255, 255]])
+    assert np.all(two[:, 8] == np.float32(np.log(np.float64(np.float32(1e-4)))))
+    with pytest.raises(O.OracleError):
+        O.gaussians_from_sfm([[np.nan, 0.0, 0.0]], [[0, 0, 0]])
+
+
+def points3d_bin(xyz, rgb, tracks):
+    """A COLMAP points3D.bin (sfm.rs:143-146): u64 count, then per point u64 id,
+    3 f64, 3 u8, f64 error, u64 track length, track length x (u32, u32)."""
+    import struct
+
+    b = struct.pack("<Q", len(xyz))
+    for k, (p, c, t) in enumerate(zip(xyz, rgb, tracks)):
+        b += struct.pack("<Q3d3BdQ", 1000 + k, *map(float, p), *map(int, c), 0.5, t)
+        b += b"".join(struct.pack("<II", k, m) for m in range(t))
+    return b
+
+
+def test_points3d_bin_parse():
+    xyz, rgb = RC.sfm_cloud(40, 12)
+    data = points3d_bin(xyz, rgb, [k % 5 for k in range(40)])
+    px, pc = O.parse_points3d_bin(data)
+    assert np.array_equal(px, xyz) and np.array_equal(pc, rgb)
+    for cut in (4, 20, len(data) - 3):
+        with pytest.raises(O.OracleError):
+            O.parse_points3d_bin(data[:cut])
