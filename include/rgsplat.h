@@ -102,6 +102,11 @@ typedef struct rgs_options {
                              flat indices 11..13, optimizer.rs:181). 0: moments follow their
                              Gaussians and lr_sh_dc applies to sh[0], sh[16], sh[32]. */
     int pixels_per_thread; /* blend kernels: 1 or 2 (default) vertically adjacent pixels */
+    uint64_t batch_pair_limit; /* pair budget of one batched launch: a batched step whose
+                                  (Gaussian, tile) pairs outgrow the pair buffer and pass this
+                                  runs as consecutive view groups within it (gradients summed
+                                  across groups, one Adam step); 0 = default 2^30 (pair buffers
+                                  and sort scratch take 16 bytes per pair) */
 } rgs_options;
 
 /* Step modes of rgs_trainer_step. */
@@ -339,6 +344,9 @@ typedef struct rgs_stats {
     uint64_t pair_capacity; /* pair buffer capacity (batched mode) */
     uint32_t graph_captures;
     uint32_t overflow_retries;
+    uint32_t view_groups;   /* groups the last batched step ran as: 1, or more
+                               when its pairs passed 2^30 (each group within it) */
+    uint32_t reserved;
 } rgs_stats;
 int rgs_get_stats(rgs_ctx* ctx, rgs_stats* out);
 

@@ -30,6 +30,8 @@ from .api import (  # noqa: F401
     render_and_backward_variant,
     render_color,
     reset_opacities,
+    camera_schedule,
+    train_blocking,
 )
 
 __version__ = "0.1.0"

@@ -106,6 +106,7 @@ class rgs_options(C.Structure):
         ("batch", C.c_int),
         ("reference_compat", C.c_int),
         ("pixels_per_thread", C.c_int),
+        ("batch_pair_limit", C.c_uint64),
     ]
 
 
@@ -116,6 +117,8 @@ class rgs_stats(C.Structure):
         ("pair_capacity", C.c_uint64),
         ("graph_captures", C.c_uint32),
         ("overflow_retries", C.c_uint32),
+        ("view_groups", C.c_uint32),
+        ("reserved", C.c_uint32),
     ]
 
 

@@ -143,7 +143,7 @@ class Context:
     """One CUDA stream plus the library's device buffers (``rgs_ctx``)."""
 
     def __init__(self, device: int = 0, tile: tuple[int, int] = (16, 16), batch: int = 256, reference_compat: bool = True,
-                 pixels_per_thread: int = 2):
+                 pixels_per_thread: int = 2, batch_pair_limit: int = 0):
         self.lib = L.load()
         o = L.rgs_options()
         self.lib.rgs_options_default(C.byref(o))
@@ -152,6 +152,7 @@ class Context:
         o.batch = int(batch)
         o.reference_compat = 1 if reference_compat else 0
         o.pixels_per_thread = int(pixels_per_thread)
+        o.batch_pair_limit = int(batch_pair_limit)
         h = C.c_void_p()
         rc = self.lib.rgs_create(C.byref(o), C.byref(h))
         if rc != L.RGS_OK:
@@ -652,3 +653,60 @@ class Trainer:
     def set_adam_state(self, state: AdamState) -> None:
         c = state.to_c()
         self.ctx.check(self.lib.rgs_trainer_set_adam_state(self.ctx.handle, C.byref(c)))
+
+
+# ---------------------------------------------------------------------------
+# the training loop
+# ---------------------------------------------------------------------------
+CAMERA_SEED = 0x9E3779B97F4A7C15
+
+
+def camera_schedule(n_cams: int, seed: int = CAMERA_SEED):
+    """``train_blocking``'s camera picker (src/pipeline/mod.rs:223-230): xorshift64
+    (x ^= x << 13; x ^= x >> 7; x ^= x << 17), then ``x % n_cams``."""
+    x = seed
+    m = (1 << 64) - 1
+    while True:
+        x ^= (x << 13) & m
+        x ^= x >> 7
+        x ^= (x << 17) & m
+        yield x % n_cams
+
+
+def train_blocking(trainer: Trainer, cfg: TrainConfig | None = None, bg=(0.0, 0.0, 0.0), loss_cfg: LossConfig | None = None,
+                   views_per_step: int = 1, mode: int | None = None, save_interval: int = 0, out_dir=None,
+                   before_densify=None, after_densify=None) -> np.ndarray:
+    """``train_blocking`` (src/pipeline/mod.rs:203-265) on a device-resident trainer.
+
+    Iterations ``0 .. cfg.num_iterations``: the next ``views_per_step`` cameras of
+    the xorshift schedule, one render + backward + Adam step (per-view launches
+    for one view unless ``mode`` says otherwise, the captured batched step for
+    several, gradients summed over the step's views); ``densify_and_prune``
+    when ``densify_from_iter <= iter <= densify_until_iter``, ``iter % 100 == 0``
+    and ``iter > 0`` with the extent of the initial Gaussians; ``reset_opacities``
+    when ``iter % opacity_reset_iter == 0``; a ``ckpt_{iter:06}.ply`` every
+    ``save_interval`` iterations into ``out_dir``. ``before_densify(iter,
+    trainer)`` / ``after_densify(iter, trainer, n)`` are called around each
+    densification. Returns each iteration's loss summed over its views."""
+    cfg = cfg or TrainConfig()
+    if mode is None:
+        mode = Trainer.PLAIN if views_per_step == 1 else Trainer.BATCHED
+    extent = estimate_scene_extent(trainer.gaussians())
+    cams = camera_schedule(len(trainer.cameras))
+    losses = np.zeros(cfg.num_iterations, np.float32)
+    if save_interval and out_dir is not None:
+        os.makedirs(out_dir, exist_ok=True)
+    for it in range(cfg.num_iterations):
+        views = [next(cams) for _ in range(views_per_step)]
+        losses[it] = np.float32(trainer.step(views, bg=bg, loss_cfg=loss_cfg, train_cfg=cfg, mode=mode).sum())
+        if cfg.densify_from_iter <= it <= cfg.densify_until_iter and it % 100 == 0 and it > 0:
+            if before_densify:
+                before_densify(it, trainer)
+            n = trainer.densify_and_prune(cfg, extent)
+            if after_densify:
+                after_densify(it, trainer, n)
+        if cfg.opacity_reset_iter and it % cfg.opacity_reset_iter == 0 and it > 0:
+            trainer.reset_opacities()
+        if save_interval and out_dir is not None and it % save_interval == 0 and it > 0:
+            trainer.save_ply(os.path.join(out_dir, f"ckpt_{it:06d}.ply"))
+    return losses

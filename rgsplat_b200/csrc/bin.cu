@@ -4,8 +4,9 @@
 // splat's index into every tile its 3-sigma rectangle touches
 // (src/cpu/backward.rs:190-205). Here the depth-sorted slot order comes from
 // sort.cu; this file turns it into pairs:
-//   count scan: exclusive scan of per-slot tile counts in depth order (the
-//               total pair count stays on the device);
+//   count scan: exclusive scan of per-slot tile counts in depth order, in
+//               64 bits (the total pair count stays on the device; a batch
+//               whose count passes 32 bits is reported, never wrapped);
 //   emit:       every block expands its chunk of depth-sorted slots into
 //               (global CTA tile id, slot) pairs, load-balanced by a binary
 //               search over the sub-tile's offsets in shared memory;
@@ -48,7 +49,7 @@ __device__ __forceinline__ void bin_chunk(uint32_t n, int G, int b, uint32_t& be
 __device__ __forceinline__ uint32_t tiles_of(uint2 d) { return (d.y & 0xffffu) * (d.y >> 16); }
 
 __global__ void __launch_bounds__(BIN_THREADS) k_count_reduce(const uint32_t* __restrict__ order, const uint32_t* __restrict__ cnt,
-                                                              uint32_t S, uint32_t* __restrict__ block_sums) {
+                                                              uint32_t S, unsigned long long* __restrict__ block_sums) {
     __shared__ uint32_t s_w[BIN_THREADS / 32];
     uint32_t begin, end;
     bin_chunk(S, gridDim.x, blockIdx.x, begin, end);
@@ -59,46 +60,73 @@ __global__ void __launch_bounds__(BIN_THREADS) k_count_reduce(const uint32_t* __
     if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = s;
     __syncthreads();
     if (threadIdx.x == 0) {
-        uint32_t t = 0;
+        unsigned long long t = 0;
         for (int w = 0; w < BIN_THREADS / 32; ++w) t += s_w[w];
         block_sums[blockIdx.x] = t;
     }
 }
 
-// Exclusive scan of the G block sums (single block); writes the total.
-__global__ void __launch_bounds__(1024) k_scan_block_sums(uint32_t* __restrict__ block_sums, int G, uint32_t* __restrict__ total) {
-    __shared__ uint32_t s[1024];
-    __shared__ uint32_t s_carry;
+// Exclusive scan of the G block sums (single block) in 64 bits; writes the
+// total to *total64 and, saturated at 2^32 - 1, to *total.
+__global__ void __launch_bounds__(1024) k_scan_block_sums(unsigned long long* __restrict__ block_sums, int G,
+                                                          uint32_t* __restrict__ total,
+                                                          unsigned long long* __restrict__ total64) {
+    __shared__ unsigned long long s[1024];
+    __shared__ unsigned long long s_carry;
     if (threadIdx.x == 0) s_carry = 0;
     __syncthreads();
     for (int base = 0; base < G; base += 1024) {
         int i = base + threadIdx.x;
-        uint32_t v = i < G ? block_sums[i] : 0u;
+        unsigned long long v = i < G ? block_sums[i] : 0ull;
         s[threadIdx.x] = v;
         __syncthreads();
         for (int o = 1; o < 1024; o <<= 1) {
-            uint32_t t = threadIdx.x >= o ? s[threadIdx.x - o] : 0u;
+            unsigned long long t = threadIdx.x >= o ? s[threadIdx.x - o] : 0ull;
             __syncthreads();
             s[threadIdx.x] += t;
             __syncthreads();
         }
-        uint32_t incl = s[threadIdx.x];
+        unsigned long long incl = s[threadIdx.x];
         if (i < G) block_sums[i] = s_carry + incl - v;
         __syncthreads();
         if (threadIdx.x == 1023) s_carry += incl;
         __syncthreads();
     }
-    if (threadIdx.x == 0) *total = s_carry;
+    if (threadIdx.x == 0) {
+        *total = s_carry > 0xffffffffull ? 0xffffffffu : (uint32_t)s_carry;
+        *total64 = s_carry;
+    }
 }
 
-void launch_count_scan(const uint32_t* order, const uint32_t* cnt, uint32_t S, uint32_t* block_sums, uint32_t* total, int grid,
-                       cudaStream_t st) {
+void launch_count_scan(const uint32_t* order, const uint32_t* cnt, uint32_t S, unsigned long long* block_sums, uint32_t* total,
+                       unsigned long long* total64, int grid, cudaStream_t st) {
     k_count_reduce<<<grid, BIN_THREADS, 0, st>>>(order, cnt, S, block_sums);
-    k_scan_block_sums<<<1, 1024, 0, st>>>(block_sums, grid, total);
+    k_scan_block_sums<<<1, 1024, 0, st>>>(block_sums, grid, total, total64);
+}
+
+__global__ void __launch_bounds__(BIN_THREADS) k_view_pairs(const uint32_t* __restrict__ cnt, uint32_t n,
+                                                            unsigned long long* __restrict__ out) {
+    __shared__ unsigned long long s_w[BIN_THREADS / 32];
+    const uint32_t* c = cnt + (size_t)blockIdx.x * n;
+    unsigned long long t = 0;
+    for (uint32_t i = threadIdx.x; i < n; i += BIN_THREADS) t += c[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long v = 0;
+        for (int w = 0; w < BIN_THREADS / 32; ++w) v += s_w[w];
+        out[blockIdx.x] = v;
+    }
+}
+
+void launch_view_pairs(const uint32_t* cnt, uint32_t n, int V, unsigned long long* out, cudaStream_t st) {
+    if (V > 0) k_view_pairs<<<V, BIN_THREADS, 0, st>>>(cnt, n, out);
 }
 
 __global__ void __launch_bounds__(BIN_THREADS) k_emit(const uint32_t* __restrict__ order, const uint2* __restrict__ tdesc, uint32_t S,
-                                                      const uint32_t* __restrict__ block_sums, uint32_t* __restrict__ pkeys,
+                                                      const unsigned long long* __restrict__ block_sums, uint32_t* __restrict__ pkeys,
                                                       uint32_t* __restrict__ pvals, uint32_t cap, int* __restrict__ overflow,
                                                       const uint32_t* __restrict__ total, uint32_t* __restrict__ eff,
                                                       const DevCam* __restrict__ cams, uint32_t n_per_view) {
@@ -113,7 +141,7 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit(const uint32_t* __restrict
     uint32_t begin, end;
     bin_chunk(S, gridDim.x, blockIdx.x, begin, end);
     if (blockIdx.x == 0 && threadIdx.x == 0) *eff = min(*total, cap);
-    uint32_t base = block_sums[blockIdx.x];
+    unsigned long long base = block_sums[blockIdx.x];
     for (uint32_t r0 = begin; r0 < end; r0 += BIN_SUB) {
         // per-thread consecutive ranks r0 + tid*PER + k
         uint32_t c[PER], local = 0;
@@ -197,7 +225,7 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit(const uint32_t* __restrict
             __syncthreads();
             const uint32_t n_round = min((uint32_t)(BIN_THREADS * EMIT_VT), sub_total - o0);
             for (uint32_t i = tid; i < n_round; i += BIN_THREADS) {
-                const uint32_t out = base + o0 + i;
+                const unsigned long long out = base + o0 + i;
                 if (out < cap) {
                     pkeys[out] = s_ek[emit_pad((int)i)];
                     pvals[out] = s_ev[emit_pad((int)i)];
@@ -222,7 +250,7 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit(const uint32_t* __restrict
 constexpr int EG = 8;
 __global__ void __launch_bounds__(BIN_THREADS) k_emit_pruned(const uint32_t* __restrict__ order, const uint2* __restrict__ tdesc,
                                                              const uint32_t* __restrict__ cnt, const float4* __restrict__ rec,
-                                                             uint32_t S, const uint32_t* __restrict__ block_sums,
+                                                             uint32_t S, const unsigned long long* __restrict__ block_sums,
                                                              uint32_t* __restrict__ pkeys, uint32_t* __restrict__ pvals,
                                                              uint32_t cap, int* __restrict__ overflow,
                                                              const uint32_t* __restrict__ total, uint32_t* __restrict__ eff,
@@ -238,7 +266,7 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit_pruned(const uint32_t* __r
     uint32_t begin, end;
     bin_chunk(S, gridDim.x, blockIdx.x, begin, end);
     if (blockIdx.x == 0 && threadIdx.x == 0) *eff = min(*total, cap);
-    uint32_t base = block_sums[blockIdx.x];
+    unsigned long long base = block_sums[blockIdx.x];
     for (uint32_t r0 = begin; r0 < end; r0 += BIN_SUB) {
         uint32_t c[PER], local = 0;
 #pragma unroll
@@ -274,7 +302,11 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit_pruned(const uint32_t* __r
         for (int k0 = 0; k0 < BIN_SUB; k0 += NGROUPS) {
             const int k = k0 + grp;
             const uint32_t nk = s_off[k + 1] - s_off[k];
-            const uint32_t out0 = base + s_off[k];
+            const unsigned long long out0 = base + s_off[k];
+            // entries of this slot's run that fit below the capacity
+            const uint32_t room = out0 >= cap ? 0u : (uint32_t)min((unsigned long long)nk, cap - out0);
+            uint32_t* const pk = pkeys + (out0 < cap ? out0 : 0ull);
+            uint32_t* const pv = pvals + (out0 < cap ? out0 : 0ull);
             uint32_t slot = 0, tbase = 0;
             int cx0 = 0, cx1 = 0, ty0 = 0, rows = 0, tiles_x = 1, height = 0;
             SpanSetup u{};
@@ -310,10 +342,9 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit_pruned(const uint32_t* __r
                 uint32_t p = written + incl - span;
                 const uint32_t key0 = tbase + (uint32_t)((ty0 + row) * tiles_x + c0);
                 for (uint32_t t = 0; t < span; ++t, ++p) {
-                    const uint32_t out = out0 + p;
-                    if (p < nk && out < cap) {
-                        pkeys[out] = key0 + t;
-                        pvals[out] = slot;
+                    if (p < room) {
+                        pk[p] = key0 + t;
+                        pv[p] = slot;
                     } else {
                         *overflow = 1;
                     }
@@ -330,7 +361,7 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit_pruned(const uint32_t* __r
 }
 
 void launch_emit_pairs(const uint32_t* order, const uint2* tdesc, const uint32_t* cnt, const float4* rec, uint32_t S,
-                       const uint32_t* block_sums, uint32_t* pair_keys, uint32_t* pair_vals, uint32_t cap, int* overflow,
+                       const unsigned long long* block_sums, uint32_t* pair_keys, uint32_t* pair_vals, uint32_t cap, int* overflow,
                        const uint32_t* total, uint32_t* eff, const DevCam* cams, uint32_t n_per_view, int tile_w,
                        int tile_h, int prune, int grid, cudaStream_t st) {
     if (prune)

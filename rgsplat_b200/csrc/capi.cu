@@ -45,7 +45,13 @@ struct StepOut {
     uint32_t visible;
     uint32_t pad;
     float losses[MAX_VIEWS];
+    unsigned long long pairs64;  // exact pair count (pairs saturates at 2^32 - 1)
 };
+
+// Default of rgs_options.batch_pair_limit: a batched step whose (Gaussian,
+// tile) pairs exceed it runs as consecutive view groups that each stay
+// within it (pair buffers and sort scratch take 16 bytes per pair: 17 GB).
+constexpr unsigned long long BATCH_PAIR_LIMIT = 1ull << 30;
 
 enum {
     SC_PAIRS = 0,
@@ -55,7 +61,8 @@ enum {
     SC_WORK_B = 4,
     SC_FINITE = 5,
     SC_VISIBLE = 6,
-    SC_COUNT = 8
+    SC_PAIRS64 = 8,  // u64 over slots 8 and 9
+    SC_COUNT = 10
 };
 
 }  // namespace
@@ -79,7 +86,7 @@ struct rgs_ctx {
     DBuf pkeys, pvals;
     uint32_t pair_cap = 0;
     DBuf ranges, rgb, final_t, last, dl, partials;
-    DBuf scalars, block_sums;
+    DBuf scalars, block_sums, view_pairs;
     SortScratch sort;
     SfmScratch sfm;
     DBuf dens_scratch, dens_out, m_tmp;
@@ -355,17 +362,19 @@ int ensure_work(rgs_ctx* ctx, size_t S, size_t px, size_t tiles, size_t lblocks,
     CK(ctx->dl.ensure(px * 3 * 4));
     CK(ctx->partials.ensure(std::max<size_t>(lblocks, 1) * 2 * 4));
     CK(ctx->scalars.ensure(SC_COUNT * 4));
-    CK(ctx->block_sums.ensure((size_t)bin_grid_blocks() * 4 + 64));
+    CK(ctx->block_sums.ensure((size_t)bin_grid_blocks() * 8 + 64));
+    CK(ctx->view_pairs.ensure(MAX_VIEWS * 8));
     CK(ctx->hdr.ensure(sizeof(StepHdr)));
     CK(ctx->outd.ensure(sizeof(StepOut)));
     (void)V;
     return RGS_OK;
 }
 
-int ensure_pairs(rgs_ctx* ctx, size_t K) {
+int ensure_pairs(rgs_ctx* ctx, unsigned long long K) {
     if (K <= ctx->pair_cap && ctx->pkeys.p) return RGS_OK;
-    size_t cap = std::max<size_t>(K + K / 4 + 1024, 1 << 16);
-    if (cap > 0xF0000000ull) return fail(ctx, RGS_ERR_CAPACITY, "more than 2^32 (Gaussian, tile) pairs");
+    if (K > 0xC0000000ull) return fail(ctx, RGS_ERR_CAPACITY, "more than 3 * 2^30 (Gaussian, tile) pairs in one view");
+    unsigned long long cap = std::max<unsigned long long>(K + K / 4 + 1024, 1 << 16);
+    cap = std::min<unsigned long long>(cap, 0xF0000000ull);
     ctx->pkeys.release();
     ctx->pvals.release();
     CK(ctx->pkeys.ensure(cap * 4));
@@ -403,11 +412,12 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
     if (e != cudaSuccess) return cuda_fail(ctx, e, "depth sort");
     mark(ctx, 2);
     const uint32_t* order = which ? ctx->sort.vals2.as<uint32_t>() : ctx->ids.as<uint32_t>();
-    launch_count_scan(order, ctx->cnt.as<uint32_t>(), (uint32_t)S, ctx->block_sums.as<uint32_t>(), sc + SC_PAIRS,
-                      bin_grid_blocks(), st);
+    launch_count_scan(order, ctx->cnt.as<uint32_t>(), (uint32_t)S, ctx->block_sums.as<unsigned long long>(), sc + SC_PAIRS,
+                      (unsigned long long*)(sc + SC_PAIRS64), bin_grid_blocks(), st);
     if (host_count) {
-        uint32_t K = 0, vis = 0;
-        CK(cudaMemcpyAsync(&K, sc + SC_PAIRS, 4, cudaMemcpyDeviceToHost, st));
+        unsigned long long K = 0;
+        uint32_t vis = 0;
+        CK(cudaMemcpyAsync(&K, sc + SC_PAIRS64, 8, cudaMemcpyDeviceToHost, st));
         if (project) CK(cudaMemcpyAsync(&vis, sc + SC_VISIBLE, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         ctx->stats.visible += vis;
@@ -435,7 +445,7 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
     }
     CK(cudaMemsetAsync(sc + SC_OVERFLOW, 0, 4, st));
     launch_emit_pairs(order, ctx->tdesc.as<uint2>(), ctx->cnt.as<uint32_t>(), ctx->rec.as<float4>(), (uint32_t)S,
-                      ctx->block_sums.as<uint32_t>(), ctx->pkeys.as<uint32_t>(), ctx->pvals.as<uint32_t>(), ctx->pair_cap,
+                      ctx->block_sums.as<unsigned long long>(), ctx->pkeys.as<uint32_t>(), ctx->pvals.as<uint32_t>(), ctx->pair_cap,
                       (int*)(sc + SC_OVERFLOW), sc + SC_PAIRS, sc + SC_PAIRS_EFF, cams_dev, (uint32_t)s.n, ctx->opt.tile_w,
                       ctx->opt.tile_h, prune ? 1 : 0, bin_grid_blocks(), st);
     mark(ctx, 3);
@@ -594,6 +604,7 @@ void rgs_options_default(rgs_options* o) {
     o->batch = 256;
     o->reference_compat = 1;
     o->pixels_per_thread = 2;
+    o->batch_pair_limit = 0;
 }
 
 void rgs_train_config_default(rgs_train_config* c) {
@@ -639,6 +650,7 @@ int rgs_create(const rgs_options* opts, rgs_ctx** out) {
         return RGS_ERR_NO_DEVICE;
     }
     if (o.device < 0 || o.device >= ndev) return RGS_ERR_INVALID_ARG;
+    if (o.batch_pair_limit == 0) o.batch_pair_limit = BATCH_PAIR_LIMIT;
     rgs_ctx* ctx = new rgs_ctx();
     ctx->opt = o;
     ctx->device = o.device;
@@ -672,7 +684,7 @@ void rgs_destroy(rgs_ctx* ctx) {
     for (auto& t : ctx->targets) t.release();
     DBuf* bufs[] = {&ctx->hdr, &ctx->outd, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->dkey, &ctx->ids, &ctx->acc, &ctx->gv, &ctx->pkeys, &ctx->pvals,
                     &ctx->ranges, &ctx->rgb, &ctx->final_t, &ctx->last, &ctx->dl, &ctx->partials, &ctx->scalars,
-                    &ctx->block_sums, &ctx->sort.hist, &ctx->sort.keys2, &ctx->sort.vals2, &ctx->dens_scratch,
+                    &ctx->block_sums, &ctx->view_pairs, &ctx->sort.hist, &ctx->sort.keys2, &ctx->sort.vals2, &ctx->dens_scratch,
                     &ctx->dens_out, &ctx->m_tmp, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->stage_d,
                     &ctx->target_stage, &ctx->tstore};
     for (DBuf* b : bufs) b->release();
@@ -1283,7 +1295,7 @@ void batch_caps(rgs_ctx* ctx, int V, size_t& px, size_t& tiles, size_t& lb) {
 }
 
 int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], float lambda, const rgs_train_config& tc,
-                    bool fused, bool host_targets) {
+                    bool fused, bool host_targets, int accumulate) {
     Scene& s = ctx->tr;
     cudaStream_t st = ctx->st;
     if (ctx->gexec) {
@@ -1328,10 +1340,11 @@ int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], fl
                                  ctx->rec.as<float4>(), ctx->gv.as<float4>(), a, st);
         } else {
             launch_geometry(s.params.as<float4>(), s.n, s.cap, cams_dev, V, ctx->cnt.as<uint32_t>(), ctx->acc.as<float4>(),
-                            ctx->rec.as<float4>(), ctx->gv.as<float4>(), s.grads.as<float4>(), 0, st);
+                            ctx->rec.as<float4>(), ctx->gv.as<float4>(), s.grads.as<float4>(), accumulate, st);
         }
         mark(ctx, 9);
         cudaMemcpyAsync(&ctx->out_h->pairs, sc + SC_PAIRS, 4, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(&ctx->out_h->pairs64, sc + SC_PAIRS64, 8, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(&ctx->out_h->overflow, sc + SC_OVERFLOW, 4, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(&ctx->out_h->visible, sc + SC_VISIBLE, 4, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(ctx->out_h->losses, losses_dev, sizeof(float) * V, cudaMemcpyDeviceToHost, st);
@@ -1352,8 +1365,12 @@ int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], fl
 
 // Batched path: one launch per stage over all views, replayed from a CUDA
 // graph; the fused geometry-backward + Adam kernel ends the step.
+int split_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], float lambda, const rgs_train_config& tc,
+               float* losses, bool fused, const float* const* host_targets);
+
 int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], float lambda, const rgs_train_config& tc,
-                 float* losses, bool fused, const float* const* host_targets = nullptr) {
+                 float* losses, bool fused, const float* const* host_targets = nullptr, int accumulate = 0,
+                 bool allow_split = true) {
     Scene& s = ctx->tr;
     StepHdr* h = ctx->hdr_h;
     for (int v = 0; v < V; ++v) {
@@ -1400,7 +1417,8 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
                                          px_cap, tiles_cap, lb_cap, (uint64_t)fused, (uint64_t)ctx->prof,
                                          (uint64_t)(uintptr_t)ctx->st, (uint64_t)ctx->opt.tile_w,
                                          (uint64_t)ctx->opt.tile_h, (uint64_t)ctx->opt.batch,
-                                         (uint64_t)ctx->opt.pixels_per_thread, (uint64_t)(host_targets != nullptr)};
+                                         (uint64_t)ctx->opt.pixels_per_thread, (uint64_t)(host_targets != nullptr),
+                                         (uint64_t)accumulate};
             for (const DBuf* b : bufs) key.push_back((uint64_t)(uintptr_t)b->p);
             for (float f : fk) {
                 uint32_t u;
@@ -1412,7 +1430,7 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
         std::vector<uint64_t> key = make_key();
         if (!ctx->gexec || key != ctx->g_key) {
             for (int i = 0; i <= RGS_NUM_STAGES; ++i) ctx->ev_marked[i] = false;
-            if ((rc = capture_batched(ctx, V, tiles_cap, bg, lambda, tc, fused, host_targets != nullptr))) {
+            if ((rc = capture_batched(ctx, V, tiles_cap, bg, lambda, tc, fused, host_targets != nullptr, accumulate))) {
                 s.t -= tstep;
                 return rc;
             }
@@ -1431,20 +1449,64 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
             for (int i = 0; i <= RGS_NUM_STAGES; ++i) ctx->ev_marked[i] = ctx->graph_marked[i];
             prof_collect(ctx);
         }
-        ctx->stats.pairs = ctx->out_h->pairs;
+        ctx->stats.pairs = ctx->out_h->pairs64;
         ctx->stats.visible = ctx->out_h->visible;
+        ctx->stats.view_groups = 1;
         if (!ctx->out_h->overflow) {
             if (losses)
                 for (int v = 0; v < V; ++v) losses[v] = ctx->out_h->losses[v];
             if (fused) s.mlen = std::max(s.mlen, s.n);
             return RGS_OK;
         }
-        // pair buffer too small: Adam was skipped on the device; grow and redo
+        // pair buffer too small: Adam was skipped on the device; grow and
+        // redo, or run the batch as view groups when it is past the limit
         s.t -= tstep;
         ctx->stats.overflow_retries += 1;
-        if ((rc = ensure_pairs(ctx, ctx->out_h->pairs))) return rc;
+        if (accumulate) return fail(ctx, RGS_ERR_CAPACITY, "a view group outgrew its pair buffer");
+        const unsigned long long K = ctx->out_h->pairs64;
+        if (K > ctx->opt.batch_pair_limit && allow_split && V > 1) return split_step(ctx, views, V, bg, lambda, tc, losses, fused, host_targets);
+        if ((rc = ensure_pairs(ctx, K))) return rc;
     }
     return fail(ctx, RGS_ERR_CAPACITY, "pair buffer overflow persisted");
+}
+
+// The batch's views in consecutive groups whose pairs stay within the
+// context's batch_pair_limit (per-view counts from the projection that just ran): each
+// group runs the batched pipeline without Adam, gradients accumulating across
+// groups, then one Adam step with denom += V -- the summed-gradient
+// semantics of a single batch.
+int split_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], float lambda, const rgs_train_config& tc,
+               float* losses, bool fused, const float* const* host_targets) {
+    Scene& s = ctx->tr;
+    unsigned long long per[MAX_VIEWS];
+    launch_view_pairs(ctx->cnt.as<uint32_t>(), (uint32_t)s.n, V, ctx->view_pairs.as<unsigned long long>(), ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(per, ctx->view_pairs.p, sizeof(unsigned long long) * V, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    int groups = 0;
+    unsigned long long total = 0;
+    for (int v0 = 0; v0 < V;) {
+        int v1 = v0 + 1;
+        unsigned long long k = per[v0];
+        while (v1 < V && k + per[v1] <= ctx->opt.batch_pair_limit) k += per[v1++];
+        // size the pair buffer for the group first: a group that accumulates
+        // into the gradients must not overflow and be redone
+        int rc = ensure_pairs(ctx, k);
+        if (rc) return rc;
+        rc = batched_step(ctx, views + v0, v1 - v0, bg, lambda, tc, losses ? losses + v0 : nullptr, false,
+                          host_targets ? host_targets + v0 : nullptr, groups > 0 ? 1 : 0, false);
+        if (rc) return rc;
+        total += ctx->stats.pairs;
+        ++groups;
+        v0 = v1;
+    }
+    ctx->stats.pairs = total;
+    ctx->stats.view_groups = (uint32_t)groups;
+    if (!fused) return RGS_OK;
+    int rc = apply_adam(ctx, tc, (uint32_t)V);
+    if (rc) return rc;
+    s.mlen = std::max(s.mlen, s.n);
+    return RGS_OK;
 }
 
 }  // namespace

@@ -151,10 +151,14 @@ inline size_t sort_hist_bytes(int grid) { return ((size_t)grid * 256 + 256) * 4;
 // bin.cu
 // Pair counts come from cnt[] (full or pruned); with prune the emission
 // expands only the tiles of each row's kept span, recomputed from the record.
-void launch_count_scan(const uint32_t* order, const uint32_t* cnt, uint32_t S, uint32_t* block_sums,
-                       uint32_t* total, int grid, cudaStream_t st);
+// block_sums: one u64 per CTA of `grid`; *total is the pair count saturated
+// at 2^32 - 1, *total64 the exact count.
+void launch_count_scan(const uint32_t* order, const uint32_t* cnt, uint32_t S, unsigned long long* block_sums,
+                       uint32_t* total, unsigned long long* total64, int grid, cudaStream_t st);
+// Per-view pair totals (slot = view * n + Gaussian) into out[0, V).
+void launch_view_pairs(const uint32_t* cnt, uint32_t n, int V, unsigned long long* out, cudaStream_t st);
 void launch_emit_pairs(const uint32_t* order, const uint2* tdesc, const uint32_t* cnt, const float4* rec, uint32_t S,
-                       const uint32_t* block_sums, uint32_t* pair_keys, uint32_t* pair_vals, uint32_t cap, int* overflow,
+                       const unsigned long long* block_sums, uint32_t* pair_keys, uint32_t* pair_vals, uint32_t cap, int* overflow,
                        const uint32_t* total, uint32_t* eff, const DevCam* cams, uint32_t n_per_view, int tile_w,
                        int tile_h, int prune, int grid, cudaStream_t st);
 int bin_grid_blocks();

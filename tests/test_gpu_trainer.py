@@ -110,6 +110,37 @@ def test_batched_pair_overflow_recovers():
     assert tb.adam_state().t == 1
 
 
+def test_batch_past_pair_limit_runs_as_view_groups():
+    """A batch whose pairs pass rgs_options.batch_pair_limit runs as view groups
+    (gradients summed across groups, one Adam step): same results as plain."""
+    # large footprints: a batch needs far more pairs than the first buffer holds
+    g, cams, targets = multi_view_scene(n=4000, seed=27, log_scale=(-1.8, 0.3))
+    tp = R.Trainer(g, cams, targets)
+    tp.step([0], mode=R.Trainer.PLAIN)
+    one_view = tp.ctx.stats()["pairs"]
+    tp = R.Trainer(g, cams, targets)
+    tb = R.Trainer(g, cams, targets, ctx=R.Context(batch_pair_limit=int(one_view * 2.5)))
+    # every batch below needs more than 2.5 views' worth of pairs
+    steps = [[0, 1, 2, 3, 4, 5], [5, 4, 3, 2, 1, 0], [1, 0, 3, 0, 1, 3]]
+    for vs in steps:
+        lp = tp.step(vs, mode=R.Trainer.PLAIN)
+        lb = tb.step(vs, mode=R.Trainer.BATCHED)
+        assert np.allclose(lp, lb, rtol=1e-4, atol=1e-7)
+        st = tb.ctx.stats()
+        assert st["view_groups"] >= 2 and st["pairs"] > tb.ctx.options()["batch_pair_limit"]
+    assert (np.abs(tp.gaussians() - tb.gaussians()) <= len(steps) * step_tolerance()[None, :]).all()
+    sa, sb = tp.adam_state(), tb.adam_state()
+    assert sa.t == sb.t == len(steps)
+    assert np.array_equal(sa.grad_denom, sb.grad_denom)
+    assert np.allclose(sa.grad_accum, sb.grad_accum, rtol=1e-3, atol=1e-9)
+    # gradients only (no Adam): the groups' gradients are summed
+    tb.backward([0, 1, 2, 3, 4, 5], mode=R.Trainer.BATCHED)
+    tp.backward([0, 1, 2, 3, 4, 5], mode=R.Trainer.PLAIN)
+    a, b = tp.grads(), tb.grads()
+    assert np.linalg.norm(a - b) <= 1e-3 * np.linalg.norm(a)
+    assert tb.ctx.stats()["view_groups"] >= 2
+
+
 @pytest.mark.parametrize("tile,ppt", [((8, 32), 2), ((32, 8), 2), ((16, 16), 1), ((32, 8), 1)])
 @pytest.mark.parametrize("batch", [128, 512])
 def test_tile_shapes_keep_reference_semantics(tile, ppt, batch):
