@@ -46,6 +46,8 @@ struct StepOut {
     uint32_t pad;
     float losses[MAX_VIEWS];
     unsigned long long pairs64;  // exact pair count (pairs saturates at 2^32 - 1)
+    int sort_fault;
+    int pad2;
 };
 
 // Default of rgs_options.batch_pair_limit: a batched step whose (Gaussian,
@@ -61,6 +63,7 @@ enum {
     SC_WORK_B = 4,
     SC_FINITE = 5,
     SC_VISIBLE = 6,
+    SC_FAULT = 7,    // sticky: a sort pass's staged copies timed out
     SC_PAIRS64 = 8,  // u64 over slots 8 and 9
     SC_COUNT = 10
 };
@@ -417,9 +420,12 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
     if (host_count) {
         unsigned long long K = 0;
         uint32_t vis = 0;
+        int fault = 0;
         CK(cudaMemcpyAsync(&K, sc + SC_PAIRS64, 8, cudaMemcpyDeviceToHost, st));
         if (project) CK(cudaMemcpyAsync(&vis, sc + SC_VISIBLE, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&fault, sc + SC_FAULT, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        if (fault) return fail(ctx, RGS_ERR_CUDA, "a sort pass's staged copies timed out");
         ctx->stats.visible += vis;
         int rc = ensure_pairs(ctx, K);
         if (rc) return rc;
@@ -550,8 +556,11 @@ int run_view_plain(rgs_ctx* ctx, Scene& s, const DevCam& dc_in, const float* tar
     mark(ctx, 6);
     CK(cudaGetLastError());
     if (rgb_host) {
+        int fault = 0;
         CK(cudaMemcpyAsync(rgb_host, ctx->rgb.p, px * 3 * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&fault, ctx->sort.fault, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        if (fault) return fail(ctx, RGS_ERR_CUDA, "a sort pass's staged copies timed out");
     }
     if (!do_backward) return RGS_OK;
     float* losses_dev = (float*)((char*)ctx->outd.p + offsetof(StepOut, losses));
@@ -575,8 +584,11 @@ int run_view_plain(rgs_ctx* ctx, Scene& s, const DevCam& dc_in, const float* tar
     mark(ctx, 9);
     CK(cudaGetLastError());
     if (loss_out) {
+        int fault = 0;
         CK(cudaMemcpyAsync(loss_out, losses_dev, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&fault, ctx->sort.fault, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        if (fault) return fail(ctx, RGS_ERR_CUDA, "a sort pass's staged copies timed out");
         prof_collect(ctx);
     }
     return RGS_OK;
@@ -660,6 +672,10 @@ int rgs_create(const rgs_options* opts, rgs_ctx** out) {
     ctx->st = ctx->own_stream;
     if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->hdr_h, sizeof(StepHdr));
     if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->out_h, sizeof(StepOut));
+    // scalar words live for the context; SC_FAULT starts (and stays) clear
+    // unless a sort pass's staged copies time out
+    if (e == cudaSuccess) e = ctx->scalars.ensure(SC_COUNT * 4);
+    if (e == cudaSuccess) e = cudaMemset(ctx->scalars.p, 0, SC_COUNT * 4);
     if (e != cudaSuccess) {
         cudaGetLastError();
         rgs_destroy(ctx);
@@ -668,6 +684,7 @@ int rgs_create(const rgs_options* opts, rgs_ctx** out) {
     std::memset(ctx->hdr_h, 0, sizeof(StepHdr));
     std::memset(ctx->out_h, 0, sizeof(StepOut));
     ctx->sort_grid = sort_grid_blocks();
+    ctx->sort.fault = ctx->scalars.as<int>() + SC_FAULT;
     *out = ctx;
     return RGS_OK;
 }
@@ -1345,6 +1362,7 @@ int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], fl
         mark(ctx, 9);
         cudaMemcpyAsync(&ctx->out_h->pairs, sc + SC_PAIRS, 4, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(&ctx->out_h->pairs64, sc + SC_PAIRS64, 8, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(&ctx->out_h->sort_fault, sc + SC_FAULT, 4, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(&ctx->out_h->overflow, sc + SC_OVERFLOW, 4, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(&ctx->out_h->visible, sc + SC_VISIBLE, 4, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(ctx->out_h->losses, losses_dev, sizeof(float) * V, cudaMemcpyDeviceToHost, st);
@@ -1449,6 +1467,7 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
             for (int i = 0; i <= RGS_NUM_STAGES; ++i) ctx->ev_marked[i] = ctx->graph_marked[i];
             prof_collect(ctx);
         }
+        if (ctx->out_h->sort_fault) return fail(ctx, RGS_ERR_CUDA, "a sort pass's staged copies timed out");
         ctx->stats.pairs = ctx->out_h->pairs64;
         ctx->stats.visible = ctx->out_h->visible;
         ctx->stats.view_groups = 1;

@@ -103,6 +103,8 @@ struct DBuf {
 struct SortScratch {
     DBuf hist;   // [G][R] u32
     DBuf keys2, vals2;
+    int* fault = nullptr;  // device word the owner provides: set (and left set)
+                           // when a pass's staged copies time out
 };
 
 // Device scratch of the SfM initialisation (sfm.cu): its own sort buffers, so

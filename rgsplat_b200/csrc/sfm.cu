@@ -165,16 +165,19 @@ int sfm_init_planes(const double* xyz, const uint8_t* rgb, int n, float4* planes
     *bad_host = 0;
     if (n <= 0) return 0;
     const size_t N = (size_t)n;
-    if ((*err = w.u32.ensure(N * 4 * 4 + 64)) != cudaSuccess) return 0;
     if ((*err = w.f64.ensure(N * 8 * 3 + 64)) != cudaSuccess) return 0;
     if ((*err = w.scales.ensure(N * 4 + 16)) != cudaSuccess) return 0;
     if ((*err = w.flag.ensure(16)) != cudaSuccess) return 0;
+    // sub-arrays on 16-byte boundaries (the sort stages full sub-tiles by bulk copy)
+    const size_t NA = (N + 3) & ~(size_t)3;
+    if ((*err = w.u32.ensure(NA * 4 * 4 + 64)) != cudaSuccess) return 0;
     uint32_t* klo = w.u32.as<uint32_t>();
-    uint32_t* khi = klo + N;
-    uint32_t* idx = khi + N;
-    uint32_t* khi2 = idx + N;
+    uint32_t* khi = klo + NA;
+    uint32_t* idx = khi + NA;
+    uint32_t* khi2 = idx + NA;
     int* bad = w.flag.as<int>();
-    if ((*err = cudaMemsetAsync(bad, 0, sizeof(int), st)) != cudaSuccess) return 0;
+    w.sort.fault = bad + 1;
+    if ((*err = cudaMemsetAsync(bad, 0, 2 * sizeof(int), st)) != cudaSuccess) return 0;
     k_sfm_keys<<<blocks(n), 256, 0, st>>>(xyz, n, klo, khi, idx, bad);
     int cur = radix_sort_pairs(klo, idx, (uint32_t)n, nullptr, 32, w.sort, grid, st, err);
     if (*err != cudaSuccess) return 0;
@@ -192,8 +195,11 @@ int sfm_init_planes(const double* xyz, const uint8_t* rgb, int n, float4* planes
     k_sfm_scales<<<blocks(n), 256, 0, st>>>(sx, sy, sz, perm, n, w.scales.as<float>());
     k_sfm_init<<<blocks(n), 256, 0, st>>>(xyz, rgb, w.scales.as<float>(), n, planes, cap);
     if ((*err = cudaGetLastError()) != cudaSuccess) return 0;
-    if ((*err = cudaMemcpyAsync(bad_host, bad, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return 0;
-    *err = cudaStreamSynchronize(st);
+    int flags[2] = {0, 0};
+    if ((*err = cudaMemcpyAsync(flags, bad, 2 * sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return 0;
+    if ((*err = cudaStreamSynchronize(st)) != cudaSuccess) return 0;
+    *bad_host = flags[0];
+    if (flags[1]) *err = cudaErrorLaunchTimeout;  // a sort pass's staged copies timed out
     return 0;
 }
 

@@ -5,14 +5,21 @@
 // the result deterministic: inputs arrive in slot order, so equal keys keep
 // index order, which is the (tile, depth bits, index) order the oracle uses.
 //
-// Each pass is reduce-then-scan with a fixed grid (no inter-block waiting, so
-// nothing can spin): every block owns one contiguous chunk of the input.
+// Each pass is reduce-then-scan with a fixed grid (no inter-block waiting):
+// every block owns one contiguous chunk of the input.
 //   upsweep:   per-block digit histogram of its chunk          -> hist[b][d]
 //   scan:      one block turns hist into global offsets (digit-major order)
 //   downsweep: each block walks its chunk in 2048-key sub-tiles, ranks keys
 //              stably (warp match_any + per-warp counters), reorders the
 //              sub-tile in shared memory by digit and writes it out with
-//              consecutive threads hitting consecutive addresses.
+//              consecutive threads hitting consecutive addresses. The next
+//              full sub-tile's keys and values arrive meanwhile by bulk copy
+//              (cp.async.bulk into the other of two shared-memory stages,
+//              completion on an mbarrier), so the block never waits on a
+//              global load; the stage that received a sub-tile then holds it
+//              reordered. The only wait is on the block's own copies, with an
+//              iteration limit: on expiry the block flags *fault, waits
+//              (bounded) for its copies in flight and stops.
 // The element count may live in device memory (pair counts are produced on
 // the GPU), so the whole sort can be captured in a CUDA graph.
 #include "rgs_internal.cuh"
@@ -128,11 +135,56 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan_hist(uint32_t* __restr
     if (lane == 0) dtot[d] = carry;
 }
 
+// ---- bulk-copy and mbarrier primitives (sm_90+ PTX) -----------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// Orders this thread's generic-proxy shared-memory accesses before later
+// async-proxy (bulk copy) writes to the same memory.
+__device__ __forceinline__ void proxy_async_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// Untiled bulk copy global -> shared (both addresses 16-byte aligned, bytes a
+// multiple of 16), completing bytes on the mbarrier. No multicast.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for phase `parity` of an mbarrier (each try_wait suspends for
+// a hardware-chosen slice): false once the limit is reached.
+constexpr int SORT_WAIT_LIMIT = 1 << 22;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (int i = 0; i < SORT_WAIT_LIMIT; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
 template <int BITS>
 __global__ void __launch_bounds__(SORT_THREADS) k_downsweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                             uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                             const uint32_t* n_dev, uint32_t n_host, int shift,
-                                                            const uint32_t* __restrict__ hist, const uint32_t* __restrict__ dtot) {
+                                                            const uint32_t* __restrict__ hist, const uint32_t* __restrict__ dtot,
+                                                            int* __restrict__ fault) {
     constexpr int R = 1 << BITS;
     constexpr int D = R / SORT_THREADS;
     __shared__ uint32_t s_run[R];
@@ -140,8 +192,11 @@ __global__ void __launch_bounds__(SORT_THREADS) k_downsweep(const uint32_t* __re
     __shared__ uint32_t s_dstart[R];
     __shared__ uint32_t s_tot[R];
     __shared__ uint32_t s_warp[SORT_WARPS];
-    __shared__ uint32_t s_keys[SORT_TILE];
-    __shared__ uint32_t s_vals[SORT_TILE];
+    // [stage][keys, values][position]: a stage receives a full sub-tile by bulk
+    // copy, then holds that sub-tile reordered by digit
+    __shared__ __align__(128) uint32_t s_stage[2][2][SORT_TILE];
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ int s_ok;
     int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     uint32_t n = load_n(n_dev, n_host), begin, end;
     chunk_of(n, gridDim.x, blockIdx.x, begin, end);
@@ -156,18 +211,62 @@ __global__ void __launch_bounds__(SORT_THREADS) k_downsweep(const uint32_t* __re
 #pragma unroll
         for (int q = 0; q < D; ++q) s_run[tid * D + q] = tb[q] + hist[(size_t)(tid * D + q) * gridDim.x + blockIdx.x];
     }
+    // sub-tiles [begin, full_end) hold SORT_TILE keys each and come by bulk
+    // copy (chunk starts are multiples of 32 keys: 128-byte aligned); a
+    // shorter last sub-tile is loaded directly
+    const uint32_t full_end = begin + (end - begin) / SORT_TILE * SORT_TILE;
+    const bool bulk_ok = ((reinterpret_cast<uintptr_t>(kin) | reinterpret_cast<uintptr_t>(vin)) & 15u) == 0;
+    const uint32_t bulk_end = bulk_ok ? full_end : begin;
+    if (tid == 0) {
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        mbar_init_fence();
+        if (begin < bulk_end) {
+            mbar_expect_tx(&s_bar[0], 2 * SORT_TILE * 4);
+            bulk_copy_g2s(s_stage[0][0], kin + begin, SORT_TILE * 4, &s_bar[0]);
+            bulk_copy_g2s(s_stage[0][1], vin + begin, SORT_TILE * 4, &s_bar[0]);
+        }
+    }
+    __syncthreads();
     const uint32_t lt_mask = (1u << lane) - 1u;
-    for (uint32_t base = begin; base < end; base += SORT_TILE) {
+    int it = 0;
+    for (uint32_t base = begin; base < end; base += SORT_TILE, ++it) {
+        const int stg = it & 1;
+        const bool staged = base < bulk_end;  // block-uniform
+        if (tid == 0 && base + SORT_TILE < bulk_end) {
+            // the other stage was last read by the previous iteration, which
+            // every thread fenced and left through a barrier
+            mbar_expect_tx(&s_bar[stg ^ 1], 2 * SORT_TILE * 4);
+            bulk_copy_g2s(s_stage[stg ^ 1][0], kin + base + SORT_TILE, SORT_TILE * 4, &s_bar[stg ^ 1]);
+            bulk_copy_g2s(s_stage[stg ^ 1][1], vin + base + SORT_TILE, SORT_TILE * 4, &s_bar[stg ^ 1]);
+        }
         for (int i = tid; i < SORT_WARPS * R; i += SORT_THREADS) (&s_wcnt[0][0])[i] = 0;
+        if (staged && tid == 0) s_ok = mbar_wait_bounded(&s_bar[stg], (uint32_t)(it >> 1) & 1u) ? 1 : 0;
         __syncthreads();
+        if (staged && !s_ok) {
+            // the copy never completed: flag it, give this block's copies in
+            // flight a bounded chance to land, and stop
+            if (tid == 0) {
+                atomicExch(fault, 1);
+                mbar_wait_bounded(&s_bar[stg], (uint32_t)(it >> 1) & 1u);
+                if (base + SORT_TILE < bulk_end) mbar_wait_bounded(&s_bar[stg ^ 1], (uint32_t)((it + 1) >> 1) & 1u);
+            }
+            return;
+        }
         uint32_t k[SORT_IPT], v[SORT_IPT], rank[SORT_IPT];
         int dig[SORT_IPT];
 #pragma unroll
         for (int i = 0; i < SORT_IPT; ++i) {
-            uint32_t pos = base + (uint32_t)(w * 32 * SORT_IPT + i * 32 + lane);
-            bool valid = pos < end;
-            k[i] = valid ? kin[pos] : 0u;
-            v[i] = valid ? vin[pos] : 0u;
+            const uint32_t local = (uint32_t)(w * 32 * SORT_IPT + i * 32 + lane);
+            const uint32_t pos = base + local;
+            const bool valid = pos < end;
+            if (staged) {
+                k[i] = s_stage[stg][0][local];
+                v[i] = s_stage[stg][1][local];
+            } else {
+                k[i] = valid ? kin[pos] : 0u;
+                v[i] = valid ? vin[pos] : 0u;
+            }
             dig[i] = valid ? (int)((k[i] >> shift) & (R - 1)) : R;
         }
 #pragma unroll
@@ -200,23 +299,26 @@ __global__ void __launch_bounds__(SORT_THREADS) k_downsweep(const uint32_t* __re
 #pragma unroll
         for (int q = 0; q < D; ++q) s_dstart[tid * D + q] = tot[q];
         __syncthreads();
+        // every thread has read this stage's keys into registers (barriers
+        // above): reorder the sub-tile into the same stage
 #pragma unroll
         for (int i = 0; i < SORT_IPT; ++i) {
             if (dig[i] < R) {
                 uint32_t lp = s_dstart[dig[i]] + s_wcnt[w][dig[i]] + rank[i];
-                s_keys[lp] = k[i];
-                s_vals[lp] = v[i];
+                s_stage[stg][0][lp] = k[i];
+                s_stage[stg][1][lp] = v[i];
             }
         }
         __syncthreads();
         uint32_t cnt = min((uint32_t)SORT_TILE, end - base);
         for (uint32_t j = tid; j < cnt; j += SORT_THREADS) {
-            uint32_t key = s_keys[j];
+            uint32_t key = s_stage[stg][0][j];
             uint32_t d = (key >> shift) & (R - 1);
             uint32_t g = s_run[d] + (j - s_dstart[d]);
             kout[g] = key;
-            vout[g] = s_vals[j];
+            vout[g] = s_stage[stg][1][j];
         }
+        proxy_async_fence();  // before this stage is refilled by bulk copy
         __syncthreads();
         for (int d = tid; d < R; d += SORT_THREADS) s_run[d] += s_tot[d];
         __syncthreads();
@@ -242,6 +344,10 @@ int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n_host, const uint
     if ((*err = sc.keys2.ensure(cap * 4 + 16)) != cudaSuccess) return 0;
     if ((*err = sc.vals2.ensure(cap * 4 + 16)) != cudaSuccess) return 0;
     if ((*err = sc.hist.ensure(sort_hist_bytes(grid))) != cudaSuccess) return 0;
+    if (!sc.fault) {
+        *err = cudaErrorInvalidValue;  // the owner provides the fault word
+        return 0;
+    }
     if (grid > 32 * SCAN_PER) {
         *err = cudaErrorInvalidValue;
         return 0;
@@ -257,7 +363,8 @@ int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n_host, const uint
         uint32_t* dtot = hist + (size_t)grid * 256;
         k_upsweep<8><<<grid, SORT_THREADS, 0, st>>>(k[cur], n_dev, n_host, shift, hist);
         k_scan_hist<8><<<256 / SCAN_WARPS, SCAN_WARPS * 32, 0, st>>>(hist, dtot, grid);
-        k_downsweep<8><<<grid, SORT_THREADS, 0, st>>>(k[cur], v[cur], k[cur ^ 1], v[cur ^ 1], n_dev, n_host, shift, hist, dtot);
+        k_downsweep<8><<<grid, SORT_THREADS, 0, st>>>(k[cur], v[cur], k[cur ^ 1], v[cur ^ 1], n_dev, n_host, shift, hist, dtot,
+                                                     sc.fault);
         cur ^= 1;
         shift += 8;
     }
