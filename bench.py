@@ -69,6 +69,7 @@ def parse_args():
     p.add_argument("--no-autotune", action="store_true", help="keep --tile/--batch/--ppt instead of autotuning")
     p.add_argument("--no-variants", action="store_true", help="skip the recompute vs store-all backward measurement")
     p.add_argument("--no-rows", action="store_true", help="skip the preview / target / model-file row measurements")
+    p.add_argument("--rows-only", action="store_true", help="measure only those rows (at --scale) and exit")
     return p.parse_args()
 
 
@@ -214,9 +215,12 @@ def measure_next_rows(R, g, cam, device: int, reps: int = 5, cpu: bool = True) -
     tmp = tempfile.mkdtemp(prefix="rgs_rows_")
     ply, splat = os.path.join(tmp, "m.ply"), os.path.join(tmp, "m.splat")
     n = g.shape[0]
+    preview = R.Trainer(g, [cam])
     rows = {
         "rasterize_srgb8": (lambda: R.rasterize(g, cam, srgb8=True, ctx=ctx), px * 4,
                             f"cpu::rasterize + to_u8_srgb, {n} Gaussians, one {cam.width}x{cam.height} view"),
+        "trainer_rasterize_srgb8": (lambda: preview.rasterize(0, srgb8=True), px * 4,
+                                    f"the same preview of a trainer's device-resident Gaussians (no upload)"),
         "target_srgb8_to_linear": (lambda: R.srgb8_to_linear(img, ctx=ctx), px * 20,
                                    f"load_target conversion, {cam.width}x{cam.height} RGBA8 -> linear f32"),
         "save_ply": (lambda: R.save_ply(g, ply, ctx=ctx), n * 248, f"io::ply::save_ply, {n} Gaussians"),
@@ -243,6 +247,7 @@ def measure_next_rows(R, g, cam, device: int, reps: int = 5, cpu: bool = True) -
         ply_bytes = open(ply, "rb").read()
         oracle_rows = {
             "rasterize_srgb8": lambda: O.to_u8_srgb(O.rasterize(g, cam)),
+            "trainer_rasterize_srgb8": lambda: O.to_u8_srgb(O.rasterize(g, cam)),
             "target_srgb8_to_linear": lambda: O.srgb8_to_linear(img.reshape(-1, 4)),
             "save_ply": lambda: open(ply + ".o", "wb").write(O.save_ply_bytes(g)),
             "save_splat": lambda: open(splat + ".o", "wb").write(O.save_splat_bytes(g)),
@@ -253,7 +258,7 @@ def measure_next_rows(R, g, cam, device: int, reps: int = 5, cpu: bool = True) -
             t0 = time.perf_counter()
             fn()
             out[name]["oracle_ms"] = round((time.perf_counter() - t0) * 1e3, 2)
-            out[name]["oracle_threads"] = threads if name == "rasterize_srgb8" else 1
+            out[name]["oracle_threads"] = threads if name.endswith("rasterize_srgb8") else 1
         del ply_bytes
     for f in (ply, splat, ply + ".o", splat + ".o"):
         if os.path.exists(f):
@@ -350,6 +355,14 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local_rank))
 
+    if args.rows_only:
+        # only the rows either side of the step (preview, target upload, model
+        # files, SfM initialisation), at this --scale: a small case to profile
+        if rank == 0:
+            cfg, g = build_workload(args.scale)
+            rows = measure_next_rows(R, g, cfg.cameras[0], local_rank, reps=1, cpu=not args.no_cpu_baseline)
+            print(json.dumps({"next_rows": rows, "n_gaussians": int(g.shape[0])}), flush=True)
+        return
     tw, th = (int(x) for x in args.tile.split("x"))
     ctx = R.Context(device=local_rank, tile=(tw, th), batch=args.batch, pixels_per_thread=args.ppt)
     stream = torch.cuda.Stream()

@@ -101,7 +101,8 @@ typedef struct rgs_options {
                              compacted on prune, optimizer.rs:97-105; "SH DC" lr applies to
                              flat indices 11..13, optimizer.rs:181). 0: moments follow their
                              Gaussians and lr_sh_dc applies to sh[0], sh[16], sh[32]. */
-    int pixels_per_thread; /* blend kernels: 1 or 2 (default) vertically adjacent pixels */
+    int pixels_per_thread; /* forward blend: 1 or 2 (default) vertically adjacent pixels per
+                              thread; the backward blend takes twice as many */
     uint64_t batch_pair_limit; /* pair budget of one batched launch: a batched step whose
                                   (Gaussian, tile) pairs outgrow the pair buffer and pass this
                                   runs as consecutive view groups within it (gradients summed
@@ -171,6 +172,9 @@ int rgs_render_color(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_c
 #define RGS_FB_RGBA8_SRGB 1
 int rgs_rasterize(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, const float bg[3], int format,
                   void* out);
+/* rgs_rasterize of the trainer's device-resident Gaussians for its camera
+ * `view` (a live preview during training: no parameter upload). */
+int rgs_trainer_rasterize(rgs_ctx* ctx, uint32_t view, const float bg[3], int format, void* out);
 
 /* cpu::backward::photometric_loss_grad (src/cpu/backward.rs:646-693). */
 int rgs_photometric_loss_grad(rgs_ctx* ctx, const float* rendered_rgb, const float* target_rgba, uint32_t width,

@@ -164,6 +164,7 @@ SIGNATURES = {
     "rgs_render_and_backward": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), FP, FP, C.POINTER(rgs_loss_config), FP, FP]),
     "rgs_render_and_backward_variant": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), FP, FP, C.POINTER(rgs_loss_config),
                                                   C.c_int, FP, FP, C.POINTER(rgs_backward_report)]),
+    "rgs_trainer_rasterize": (C.c_int, [CTX, C.c_uint32, FP, C.c_int, C.c_void_p]),
     "rgs_rasterize": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), FP, C.c_int, C.c_void_p]),
     "rgs_render_color": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), FP, FP]),
     "rgs_photometric_loss_grad": (C.c_int, [CTX, FP, FP, C.c_uint32, C.c_uint32, C.c_float, FP, FP]),

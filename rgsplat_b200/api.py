@@ -634,6 +634,15 @@ class Trainer:
         self.ctx.check(self.lib.rgs_trainer_render(self.ctx.handle, int(view), _fp(_f32(bg)), _fp(out)))
         return out
 
+    def rasterize(self, view: int, bg=(0.0, 0.0, 0.0), srgb8: bool = False) -> np.ndarray:
+        """``cpu::rasterize`` of the device-resident Gaussians for camera ``view``:
+        RGBA float32 (H, W, 4), or with srgb8 the ``to_u8_srgb`` bytes."""
+        c = self.cameras[view]
+        out = np.zeros((c.height, c.width, 4), np.uint8 if srgb8 else np.float32)
+        fmt = L.RGS_FB_RGBA8_SRGB if srgb8 else L.RGS_FB_RGBA_F32
+        self.ctx.check(self.lib.rgs_trainer_rasterize(self.ctx.handle, int(view), _fp(_f32(bg)), int(fmt), out.ctypes.data))
+        return out
+
     def densify_and_prune(self, train_cfg: TrainConfig, scene_extent: float) -> int:
         n = C.c_size_t(0)
         tc = train_cfg.to_c()

@@ -277,11 +277,12 @@ __device__ __forceinline__ void red_add_v4(float4* addr, float x, float y, float
 // relative of the reference's, far inside the gradients' 1e-3 tolerance.
 // Alpha itself is recomputed bit for bit as the forward did, so the set of
 // contributing splats is the forward's.
-// With two pixels per thread the register budget is capped so that eight
-// 128-thread CTAs fit an SM (a few spilled words cost less than the lost
-// occupancy: measured ~2 % faster on the 1M-Gaussian step).
+// The register budget is capped for occupancy: eight 128-thread CTAs per SM
+// with two pixels per thread, twelve 64-thread CTAs with four (a few spilled
+// words cost less than the lost warps: measured 2 % and 10 % faster backward
+// passes on the 1M-Gaussian step).
 template <int TW, int TH, int BATCH, bool RECT, int PPT, bool STORE = false>
-__global__ void __launch_bounds__(TW * TH / PPT, PPT == 2 ? 8 : 1) k_blend_bwd(BlendArgs a) {
+__global__ void __launch_bounds__(TW * TH / PPT, PPT == 2 ? 8 : PPT == 4 ? 12 : 1) k_blend_bwd(BlendArgs a) {
     constexpr int NT = TW * TH / PPT;
     constexpr int NACC = 9;
     __shared__ float4 s_a[BATCH];
@@ -446,10 +447,14 @@ __global__ void __launch_bounds__(TW * TH / PPT, PPT == 2 ? 8 : 1) k_blend_bwd(B
 // ---- launch plumbing -----------------------------------------------------
 typedef void (*BlendKernel)(BlendArgs);
 
+// The forward runs `pixels_per_thread` (1 or 2) pixels per thread, the
+// backward twice that: its per-splat warp reduction is then shared by twice
+// the pixels (measured 3 % faster at 4 than at 2 on the 1M-Gaussian step,
+// while the forward is slower at 4).
 template <int TW, int TH, int BATCH, bool RECT>
 static BlendKernel pick(bool fwd, int ppt) {
-    if (ppt == 1) return fwd ? (BlendKernel)k_blend_fwd<TW, TH, BATCH, RECT, 1> : (BlendKernel)k_blend_bwd<TW, TH, BATCH, RECT, 1>;
-    return fwd ? (BlendKernel)k_blend_fwd<TW, TH, BATCH, RECT, 2> : (BlendKernel)k_blend_bwd<TW, TH, BATCH, RECT, 2>;
+    if (fwd) return ppt == 1 ? (BlendKernel)k_blend_fwd<TW, TH, BATCH, RECT, 1> : (BlendKernel)k_blend_fwd<TW, TH, BATCH, RECT, 2>;
+    return ppt == 2 ? (BlendKernel)k_blend_bwd<TW, TH, BATCH, RECT, 2> : (BlendKernel)k_blend_bwd<TW, TH, BATCH, RECT, 4>;
 }
 
 template <int TW, int TH, bool RECT>
@@ -485,7 +490,7 @@ static int grid_for(BlendKernel k, int threads) {
 
 static void launch(const BlendArgs& a, int tw, int th, int batch, bool fwd, cudaStream_t st) {
     bool rect = a.rect_filter != 0 || !(tw == REF_TILE && th == REF_TILE);
-    int ppt = a.pixels_per_thread == 1 ? 1 : 2;
+    int ppt = (a.pixels_per_thread == 1 ? 1 : 2) * (fwd ? 1 : 2);
     BlendKernel k = select_kernel(tw, th, batch, rect, fwd, ppt);
     int threads = tw * th / ppt;
     cudaMemsetAsync(a.work, 0, sizeof(uint32_t), st);

@@ -852,17 +852,12 @@ int rgs_render_color(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_c
     return run_view_plain(ctx, s, dc, nullptr, bg, 0.0f, false, false, nullptr, rgb_out);
 }
 
-int rgs_rasterize(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, const float bg[3], int format,
-                  void* out) {
-    int rc = check_ctx(ctx);
-    if (rc) return rc;
-    if (!camera || !bg || !out || (n && !gaussians)) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
+// cpu::rasterize of scene s for one camera into a host framebuffer.
+int rasterize_scene(rgs_ctx* ctx, Scene& s, const rgs_camera* camera, const float bg[3], int format, void* out) {
+    int rc;
     if (format != RGS_FB_RGBA_F32 && format != RGS_FB_RGBA8_SRGB) return fail(ctx, RGS_ERR_INVALID_ARG, "unknown framebuffer format");
     DevCam dc;
     if ((rc = make_devcam(ctx, *camera, dc))) return rc;
-    Scene& s = ctx->sc;
-    if ((rc = upload_gaussians(ctx, s, gaussians, n))) return rc;
-    if ((rc = check_finite(ctx, s))) return rc;
     ctx->stats = rgs_stats{};
     if ((rc = run_view_plain(ctx, s, dc, nullptr, bg, 0.0f, false, false, nullptr, nullptr, nullptr, true))) return rc;
     const size_t px = (size_t)camera->width * camera->height;
@@ -874,6 +869,24 @@ int rgs_rasterize(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_came
     CK(cudaMemcpyAsync(out, ctx->stage_a.p, bytes, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     return RGS_OK;
+}
+
+int rgs_rasterize(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, const float bg[3], int format,
+                  void* out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!camera || !bg || !out || (n && !gaussians)) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
+    Scene& s = ctx->sc;
+    if ((rc = upload_gaussians(ctx, s, gaussians, n))) return rc;
+    if ((rc = check_finite(ctx, s))) return rc;
+    return rasterize_scene(ctx, s, camera, bg, format, out);
+}
+
+int rgs_trainer_rasterize(rgs_ctx* ctx, uint32_t view, const float bg[3], int format, void* out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!bg || !out || view >= ctx->cams.size()) return fail(ctx, RGS_ERR_INVALID_ARG, "bad argument");
+    return rasterize_scene(ctx, ctx->tr, &ctx->cams[view], bg, format, out);
 }
 
 int rgs_photometric_loss_grad(rgs_ctx* ctx, const float* rendered_rgb, const float* target_rgba, uint32_t width,

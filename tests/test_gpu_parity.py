@@ -315,3 +315,18 @@ def test_rasterize_matches_oracle(ctx, bg):
         f"max diff {np.abs(fb - ofb).max()}"
     u8 = R.rasterize(g, cam, bg, srgb8=True, ctx=ctx)
     assert np.array_equal(u8, O.to_u8_srgb(ofb))
+
+
+@pytest.mark.parametrize("bg", [(0.0, 0.0, 0.0), (0.1, 0.3, 0.5)])
+def test_trainer_rasterize_matches_oracle(bg):
+    """The trainer's device-resident Gaussians previewed without an upload: the
+    same framebuffer as rasterizing a host copy, before and after a step."""
+    g, cam, target = small_scene(seed=13, w=176, h=120)
+    tr = R.Trainer(g, [cam], [target])
+    fb = tr.rasterize(0, bg)
+    assert np.array_equal(fb.reshape(-1).view(np.uint32), O.rasterize(g, cam, bg).reshape(-1).view(np.uint32))
+    tr.step([0])
+    g2 = tr.gaussians()
+    fb2 = tr.rasterize(0, bg)
+    assert np.array_equal(fb2.reshape(-1).view(np.uint32), O.rasterize(g2, cam, bg).reshape(-1).view(np.uint32))
+    assert np.array_equal(tr.rasterize(0, bg, srgb8=True), O.to_u8_srgb(fb2))
