@@ -254,6 +254,7 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit_pruned(const uint32_t* __r
                                                              uint32_t* __restrict__ pkeys, uint32_t* __restrict__ pvals,
                                                              uint32_t cap, int* __restrict__ overflow,
                                                              const uint32_t* __restrict__ total, uint32_t* __restrict__ eff,
+                                                             const unsigned long long* __restrict__ total64,
                                                              const DevCam* __restrict__ cams, uint32_t n_per_view, int tile_w,
                                                              int tile_h) {
     __shared__ uint32_t s_off[BIN_SUB + 1];
@@ -267,6 +268,10 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit_pruned(const uint32_t* __r
     bin_chunk(S, gridDim.x, blockIdx.x, begin, end);
     if (blockIdx.x == 0 && threadIdx.x == 0) *eff = min(*total, cap);
     unsigned long long base = block_sums[blockIdx.x];
+    // culled slots sort last (depth key ~0), so whole chunks of the depth
+    // order emit nothing: such a block leaves at once
+    const unsigned long long block_end = blockIdx.x + 1 < gridDim.x ? block_sums[blockIdx.x + 1] : *total64;
+    if (block_end == base) return;
     for (uint32_t r0 = begin; r0 < end; r0 += BIN_SUB) {
         uint32_t c[PER], local = 0;
 #pragma unroll
@@ -299,6 +304,7 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit_pruned(const uint32_t* __r
         }
         if (tid == 0) s_off[BIN_SUB] = sub_total;
         __syncthreads();
+        if (sub_total == 0) continue;  // block-uniform; s_w was read before the barrier
         for (int k0 = 0; k0 < BIN_SUB; k0 += NGROUPS) {
             const int k = k0 + grp;
             const uint32_t nk = s_off[k + 1] - s_off[k];
@@ -362,11 +368,11 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit_pruned(const uint32_t* __r
 
 void launch_emit_pairs(const uint32_t* order, const uint2* tdesc, const uint32_t* cnt, const float4* rec, uint32_t S,
                        const unsigned long long* block_sums, uint32_t* pair_keys, uint32_t* pair_vals, uint32_t cap, int* overflow,
-                       const uint32_t* total, uint32_t* eff, const DevCam* cams, uint32_t n_per_view, int tile_w,
-                       int tile_h, int prune, int grid, cudaStream_t st) {
+                       const uint32_t* total, const unsigned long long* total64, uint32_t* eff, const DevCam* cams,
+                       uint32_t n_per_view, int tile_w, int tile_h, int prune, int grid, cudaStream_t st) {
     if (prune)
         k_emit_pruned<<<grid, BIN_THREADS, 0, st>>>(order, tdesc, cnt, rec, (uint32_t)S, block_sums, pair_keys, pair_vals, cap,
-                                                    overflow, total, eff, cams, n_per_view, tile_w, tile_h);
+                                                    overflow, total, eff, total64, cams, n_per_view, tile_w, tile_h);
     else
         k_emit<<<grid, BIN_THREADS, 0, st>>>(order, tdesc, S, block_sums, pair_keys, pair_vals, cap, overflow, total, eff, cams,
                                              n_per_view);

@@ -452,7 +452,8 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
     CK(cudaMemsetAsync(sc + SC_OVERFLOW, 0, 4, st));
     launch_emit_pairs(order, ctx->tdesc.as<uint2>(), ctx->cnt.as<uint32_t>(), ctx->rec.as<float4>(), (uint32_t)S,
                       ctx->block_sums.as<unsigned long long>(), ctx->pkeys.as<uint32_t>(), ctx->pvals.as<uint32_t>(), ctx->pair_cap,
-                      (int*)(sc + SC_OVERFLOW), sc + SC_PAIRS, sc + SC_PAIRS_EFF, cams_dev, (uint32_t)s.n, ctx->opt.tile_w,
+                      (int*)(sc + SC_OVERFLOW), sc + SC_PAIRS, (const unsigned long long*)(sc + SC_PAIRS64), sc + SC_PAIRS_EFF,
+                      cams_dev, (uint32_t)s.n, ctx->opt.tile_w,
                       ctx->opt.tile_h, prune ? 1 : 0, bin_grid_blocks(), st);
     mark(ctx, 3);
     int which2 = radix_sort_pairs(ctx->pkeys.as<uint32_t>(), ctx->pvals.as<uint32_t>(), ctx->pair_cap, sc + SC_PAIRS_EFF,

@@ -161,8 +161,8 @@ void launch_count_scan(const uint32_t* order, const uint32_t* cnt, uint32_t S, u
 void launch_view_pairs(const uint32_t* cnt, uint32_t n, int V, unsigned long long* out, cudaStream_t st);
 void launch_emit_pairs(const uint32_t* order, const uint2* tdesc, const uint32_t* cnt, const float4* rec, uint32_t S,
                        const unsigned long long* block_sums, uint32_t* pair_keys, uint32_t* pair_vals, uint32_t cap, int* overflow,
-                       const uint32_t* total, uint32_t* eff, const DevCam* cams, uint32_t n_per_view, int tile_w,
-                       int tile_h, int prune, int grid, cudaStream_t st);
+                       const uint32_t* total, const unsigned long long* total64, uint32_t* eff, const DevCam* cams,
+                       uint32_t n_per_view, int tile_w, int tile_h, int prune, int grid, cudaStream_t st);
 int bin_grid_blocks();
 void launch_tile_ranges(const uint32_t* pair_keys, const uint32_t* total, uint32_t cap, uint2* ranges,
                         cudaStream_t st);
