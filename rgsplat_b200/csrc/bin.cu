@@ -246,8 +246,10 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit(const uint32_t* __restrict
 // lanes, one lane per rectangle row (EG rows at a time): the lanes compute
 // their rows' spans, a group scan turns the span lengths into offsets, and
 // every lane writes its row's run of consecutive pairs. The warp's groups
-// step together for the tallest of their rectangles.
-constexpr int EG = 8;
+// step together for the tallest of their rectangles. Four lanes per slot:
+// most rectangles are a few rows tall, so eight left half the lanes idle
+// (measured 12 % slower).
+constexpr int EG = 4;
 __global__ void __launch_bounds__(BIN_THREADS) k_emit_pruned(const uint32_t* __restrict__ order, const uint2* __restrict__ tdesc,
                                                              const uint32_t* __restrict__ cnt, const float4* __restrict__ rec,
                                                              uint32_t S, const unsigned long long* __restrict__ block_sums,
