@@ -138,7 +138,7 @@ def test_batch_past_pair_limit_runs_as_view_groups():
     sa, sb = tp.adam_state(), tb.adam_state()
     assert sa.t == sb.t == len(steps)
     assert np.array_equal(sa.grad_denom, sb.grad_denom)
-    assert np.allclose(sa.grad_accum, sb.grad_accum, rtol=1e-3, atol=1e-9)
+    assert np.allclose(sa.grad_accum, sb.grad_accum, rtol=1e-3, atol=1e-6 * float(np.abs(sa.grad_accum).max()))
     # gradients only (no Adam): the groups' gradients are summed
     tb.backward([0, 1, 2, 3, 4, 5], mode=R.Trainer.BATCHED)
     tp.backward([0, 1, 2, 3, 4, 5], mode=R.Trainer.PLAIN)
