@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(TW * TH / PPT, PPT == 2 ? 8 : PPT == 4 ? 12 : 
         const float y0c = (float)(ty * TH) + 0.5f, y1c = (float)(min(ty * TH + TH, c.height) - 1) + 0.5f;
         const uint2 rg = a.ranges[tile];
         int lc[PPT];
-        float T[PPT], dl0[PPT], dl1[PPT], dl2[PPT], be0[PPT], be1[PPT], be2[PPT], pyc[PPT];
+        float T[PPT], dl0[PPT], dl1[PPT], dl2[PPT], sbe[PPT], pyc[PPT];
         int my_maxlc = -1;
 #pragma unroll
         for (int p = 0; p < PPT; ++p) {
@@ -335,9 +335,8 @@ __global__ void __launch_bounds__(TW * TH / PPT, PPT == 2 ? 8 : PPT == 4 ? 12 : 
                 dl1[p] = a.dl[pix * 3 + 1];
                 dl2[p] = a.dl[pix * 3 + 2];
             }
-            be0[p] = T[p] * a.bg[0];
-            be1[p] = T[p] * a.bg[1];
-            be2[p] = T[p] * a.bg[2];
+            // dL/dpixel . (colour behind the current splat), behind = T_final * bg
+            sbe[p] = __fmaf_rn(dl2[p], T[p] * a.bg[2], __fmaf_rn(dl1[p], T[p] * a.bg[1], dl0[p] * (T[p] * a.bg[0])));
             my_maxlc = max(my_maxlc, lc[p]);
         }
         const int warp_maxlc = __reduce_max_sync(0xffffffffu, my_maxlc);
@@ -369,6 +368,7 @@ __global__ void __launch_bounds__(TW * TH / PPT, PPT == 2 ? 8 : PPT == 4 ? 12 : 
                     const float t2b = 2.0f * Q.y * dx;
                     // per-entry factors of the conic / mean gradients
                     const float hdxx = -0.5f * dx * dx, qxdx = Q.x * dx, qydx = Q.y * dx;
+                    float su = 0.0f, sud = 0.0f, sudd = 0.0f;  // sums over pixels of u, u dy, u dy^2
 #pragma unroll
                     for (int p = 0; p < PPT; ++p) {
                         if (li > lc[p]) continue;
@@ -390,26 +390,33 @@ __global__ void __launch_bounds__(TW * TH / PPT, PPT == 2 ? 8 : PPT == 4 ? 12 : 
                             inv_1ma = __fdividef(1.0f, 1.0f - alpha);
                             T[p] = T[p] * inv_1ma;
                         }
-                        // gradient terms of backward.rs:453-484, as fused multiply-adds
+                        // gradient terms of backward.rs:453-484, as fused multiply-adds.
+                        // The colour behind enters only as dL/dpixel . behind, so one
+                        // scalar per pixel (sbe) replaces the three channels; the conic
+                        // and mean terms are linear in u = dL/dpower per pixel, so the
+                        // thread sums u, u dy and u dy^2 over its pixels and forms the
+                        // five terms once per splat (dx is the thread's column).
                         const float weight = alpha * T[p];
                         g[0] = __fmaf_rn(dl0[p], weight, g[0]);
                         g[1] = __fmaf_rn(dl1[p], weight, g[1]);
                         g[2] = __fmaf_rn(dl2[p], weight, g[2]);
-                        float dl_dalpha = dl0[p] * __fmaf_rn(T[p], K.x, -be0[p] * inv_1ma);
-                        dl_dalpha = __fmaf_rn(dl1[p], __fmaf_rn(T[p], K.y, -be1[p] * inv_1ma), dl_dalpha);
-                        dl_dalpha = __fmaf_rn(dl2[p], __fmaf_rn(T[p], K.z, -be2[p] * inv_1ma), dl_dalpha);
+                        const float dk = __fmaf_rn(dl2[p], K.z, __fmaf_rn(dl1[p], K.y, dl0[p] * K.x));
+                        const float dl_dalpha = __fmaf_rn(T[p], dk, -sbe[p] * inv_1ma);
+                        sbe[p] = __fmaf_rn(weight, dk, sbe[p]);
                         const float dl_draw = alpha_raw > 0.99f ? 0.0f : dl_dalpha;
                         g[3] = __fmaf_rn(dl_draw, g_exp, g[3]);
-                        const float dl_dpower = dl_draw * A.z * g_exp;
-                        g[4] = __fmaf_rn(dl_dpower, hdxx, g[4]);
-                        g[5] = __fmaf_rn(dl_dpower, -dx * dy, g[5]);
-                        g[6] = __fmaf_rn(dl_dpower, -0.5f * dy * dy, g[6]);
-                        g[7] = __fmaf_rn(dl_dpower, __fmaf_rn(Q.y, dy, qxdx), g[7]);
-                        g[8] = __fmaf_rn(dl_dpower, __fmaf_rn(Q.z, dy, qydx), g[8]);
-                        be0[p] = __fmaf_rn(weight, K.x, be0[p]);
-                        be1[p] = __fmaf_rn(weight, K.y, be1[p]);
-                        be2[p] = __fmaf_rn(weight, K.z, be2[p]);
+                        const float u = dl_draw * alpha_raw;
+                        su += u;
+                        sud = __fmaf_rn(u, dy, sud);
+                        sudd = __fmaf_rn(u * dy, dy, sudd);
                         contrib = true;
+                    }
+                    if (contrib) {
+                        g[4] = hdxx * su;
+                        g[5] = -dx * sud;
+                        g[6] = -0.5f * sudd;
+                        g[7] = __fmaf_rn(Q.y, sud, qxdx * su);
+                        g[8] = __fmaf_rn(Q.z, sud, qydx * su);
                     }
                 }
                 const unsigned cm = __ballot_sync(0xffffffffu, contrib);
