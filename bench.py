@@ -86,6 +86,38 @@ class ClockSampler:
         self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{device}.csv")
 
     def start(self):
+        # NVML read every 10 ms from a thread (the timed region can be a few
+        # hundred ms); nvidia-smi at its 200 ms floor otherwise. Read-only.
+        self.samples, self.nvml = [], None
+        try:
+            import threading
+
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+            bits = {"hw_slowdown": pynvml.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": pynvml.nvmlClocksEventReasonSwPowerCap}
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self.stop_ev = threading.Event()
+
+            def run():
+                while not self.stop_ev.is_set():
+                    try:
+                        mhz = float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                        r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.samples.append((mhz, [k for k, b in bits.items() if r & b]))
+                    except Exception:
+                        pass
+                    self.stop_ev.wait(0.01)
+
+            self.nvml = threading.Thread(target=run, daemon=True)
+            self.nvml.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.fh = open(self.path, "w")
@@ -95,6 +127,13 @@ class ClockSampler:
             self.proc = None
 
     def stop(self) -> dict:
+        if self.nvml is not None:
+            self.stop_ev.set()
+            self.nvml.join(timeout=2)
+            sm = [m for m, _ in self.samples]
+            reasons = sorted({r for _, rs in self.samples for r in rs})
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                    "samples": len(sm), "source": "nvml, 10 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
         self.proc.terminate()
