@@ -219,6 +219,18 @@ def profiled_traffic(kernel_file: str):
         return None
 
 
+def profiled_issue_active(kernel_prefix: str):
+    """Fraction of issue slots a kernel kept busy, from the committed ncu table
+    of the step's kernels (half-size capture of the same launch shape)."""
+    try:
+        for line in open(os.path.join(ROOT, "profiles", "step_kernels_500k_8views.md")):
+            if line.startswith(f"| `{kernel_prefix}"):
+                return round(float(line.split("|")[5]) / 100.0, 3)
+    except (OSError, ValueError, IndexError):
+        pass
+    return None
+
+
 def measure_backward_variants(R, scenes, device: int, reps: int = 5) -> dict:
     """Differentiation workload (50k Gaussians, one 512x512 view): the
     recompute-from-final-T backward against the store-all-T variant, blend
@@ -573,8 +585,10 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         roofline = {"bound": "hbm", "kernel": dom, "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
                     "frac": round(ach / hbm, 4), "peak_source": peak_src, "traffic": traffic,
                     "algorithmic_bytes": int(b),
-                    "note": "the blend kernels are bound by FP32 instruction issue (ncu: ~80-94 % issue-active, "
-                            "DRAM ~1 % of peak); the HBM fraction is reported as the contract asks"}
+                    "issue_active": profiled_issue_active("k_blend_bwd") if dom == "backward" else None,
+                    "note": "the blend kernels are bound by FP32 instruction issue (issue_active: fraction of issue "
+                            "slots busy, ncu, profiles/step_kernels_500k_8views.md; DRAM ~1 % of peak); the HBM "
+                            "fraction is reported as the contract asks"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
