@@ -88,6 +88,7 @@ struct rgs_ctx {
     DBuf rec, cnt, tdesc, dkey, ids, acc, gv;
     DBuf pkeys, pvals;
     uint32_t pair_cap = 0;
+    bool split_hint = false;  // the last batched step ran as view groups
     DBuf ranges, rgb, final_t, last, dl, partials;
     DBuf scalars, block_sums, view_pairs;
     SortScratch sort;
@@ -1431,6 +1432,27 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
         CK(ctx->target_batch.ensure(px_cap * 16));
         for (int v = 0; v < V; ++v) h->cams[v].target = ctx->target_batch.as<float>() + (size_t)h->cams[v].pix_base * 4;
     }
+    if (ctx->split_hint && allow_split && V > 1) {
+        // The last batched step ran as view groups: project this batch alone
+        // first (no emission, no blend) and, if its pairs are again past the
+        // budget, go to the groups directly instead of through a full attempt
+        // that would overflow its pair buffer.
+        const DevCam* cams_dev = (const DevCam*)((char*)ctx->hdr.p + offsetof(StepHdr, cams));
+        uint32_t* sc = ctx->scalars.as<uint32_t>();
+        CK(cudaMemcpyAsync(ctx->hdr.p, ctx->hdr_h, sizeof(StepHdr), cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemsetAsync(sc + SC_VISIBLE, 0, 4, ctx->st));
+        launch_project(s.params.as<float4>(), s.n, s.cap, cams_dev, V, ctx->opt.tile_w, ctx->opt.tile_h, ctx->rec.as<float4>(),
+                       ctx->cnt.as<uint32_t>(), ctx->tdesc.as<uint2>(), ctx->dkey.as<uint32_t>(), ctx->ids.as<uint32_t>(),
+                       zero_bg(bg) ? 1 : 0, sc + SC_VISIBLE, ctx->st);
+        launch_view_pairs(ctx->cnt.as<uint32_t>(), (uint32_t)s.n, V, ctx->view_pairs.as<unsigned long long>(), ctx->st);
+        CK(cudaGetLastError());
+        unsigned long long per[MAX_VIEWS], total = 0;
+        CK(cudaMemcpyAsync(per, ctx->view_pairs.p, sizeof(unsigned long long) * V, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        for (int v = 0; v < V; ++v) total += per[v];
+        if (total > ctx->opt.batch_pair_limit) return split_step(ctx, views, V, bg, lambda, tc, losses, fused, host_targets);
+        ctx->split_hint = false;
+    }
     const uint64_t tstep = fused ? 1 : 0;
     for (int attempt = 0; attempt < 4; ++attempt) {
         s.t += tstep;
@@ -1511,6 +1533,7 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
 int split_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], float lambda, const rgs_train_config& tc,
                float* losses, bool fused, const float* const* host_targets) {
     Scene& s = ctx->tr;
+    ctx->split_hint = true;
     unsigned long long per[MAX_VIEWS];
     launch_view_pairs(ctx->cnt.as<uint32_t>(), (uint32_t)s.n, V, ctx->view_pairs.as<unsigned long long>(), ctx->st);
     CK(cudaGetLastError());
