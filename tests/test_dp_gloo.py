@@ -81,6 +81,12 @@ def _rank(rank, world, port, out_dir):
         np.save(os.path.join(out_dir, f"params_{rank}.npy"), tr.g)
         np.save(os.path.join(out_dir, f"denom_{rank}.npy"), tr.state.grad_denom)
         np.save(os.path.join(out_dir, f"accum_{rank}.npy"), tr.state.grad_accum)
+        # densification needs no exchange either: every rank holds the same
+        # all-reduced statistics and parameters, so each densifies identically
+        avg = tr.state.grad_accum / np.maximum(tr.state.grad_denom, 1)
+        cfg = tr.O.TrainConfig(densify_grad_threshold=float(np.quantile(avg, 0.5)))
+        dens = tr.O.densify_and_prune(tr.g, tr.state, cfg, tr.O.estimate_scene_extent(g))
+        np.save(os.path.join(out_dir, f"densified_{rank}.npy"), dens)
     finally:
         dist.destroy_process_group()
 
@@ -101,6 +107,8 @@ def test_view_parallel_step_matches_single_process(tmp_path):
     # the ranks hold bit-identical parameters without any broadcast
     assert np.array_equal(p[0].view(np.uint32), p[1].view(np.uint32))
     assert np.array_equal(np.load(tmp_path / "denom_0.npy"), np.load(tmp_path / "denom_1.npy"))
+    d = [np.load(tmp_path / f"densified_{r}.npy") for r in range(world)]
+    assert d[0].shape[0] > p[0].shape[0] and np.array_equal(d[0].view(np.uint32), d[1].view(np.uint32))
 
     # one process, all 8 views per step
     g, cams, targets = scene()
