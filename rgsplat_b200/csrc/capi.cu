@@ -86,6 +86,7 @@ struct rgs_ctx {
     StepOut* out_h = nullptr;  // pinned
     DBuf outd;      // StepOut (device)
     DBuf rec, cnt, tdesc, dkey, ids, acc, gv;
+    DBuf gcache;  // per-Gaussian view-independent projection terms, [2][cap] float4
     DBuf pkeys, pvals;
     uint32_t pair_cap = 0;
     bool split_hint = false;  // the last batched step ran as view groups
@@ -374,6 +375,13 @@ int ensure_work(rgs_ctx* ctx, size_t S, size_t px, size_t tiles, size_t lblocks,
     return RGS_OK;
 }
 
+// The projection's per-Gaussian term cache for scene s (allocated outside
+// any stream capture).
+int ensure_gcache(rgs_ctx* ctx, const Scene& s) {
+    CK(ctx->gcache.ensure((size_t)std::max(s.cap, 1) * 2 * sizeof(float4)));
+    return RGS_OK;
+}
+
 int ensure_pairs(rgs_ctx* ctx, unsigned long long K) {
     if (K <= ctx->pair_cap && ctx->pkeys.p) return RGS_OK;
     if (K > 0xC0000000ull) return fail(ctx, RGS_ERR_CAPACITY, "more than 3 * 2^30 (Gaussian, tile) pairs in one view");
@@ -407,7 +415,7 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
         cudaMemsetAsync(sc + SC_VISIBLE, 0, 4, st);
         launch_project(s.params.as<float4>(), s.n, s.cap, cams_dev, V, ctx->opt.tile_w, ctx->opt.tile_h,
                        ctx->rec.as<float4>(), ctx->cnt.as<uint32_t>(), ctx->tdesc.as<uint2>(), ctx->dkey.as<uint32_t>(),
-                       ctx->ids.as<uint32_t>(), prune ? 1 : 0, sc + SC_VISIBLE, st);
+                       ctx->ids.as<uint32_t>(), prune ? 1 : 0, sc + SC_VISIBLE, ctx->gcache.as<float4>(), st);
     }
     mark(ctx, 1);
     cudaError_t e;
@@ -533,6 +541,7 @@ int run_view_plain(rgs_ctx* ctx, Scene& s, const DevCam& dc_in, const float* tar
     if (rc) return rc;
     DevCam* cams_dev;
     if ((rc = upload_single_cam(ctx, dc, &cams_dev))) return rc;
+    if ((rc = ensure_gcache(ctx, s))) return rc;
     mark(ctx, 0);
     Binned b;
     if ((rc = bin_batch(ctx, s, cams_dev, 1, tiles, true, b, true, zero_bg(bg)))) return rc;
@@ -582,7 +591,8 @@ int run_view_plain(rgs_ctx* ctx, Scene& s, const DevCam& dc_in, const float* tar
     }
     mark(ctx, 8);
     launch_geometry(s.params.as<float4>(), s.n, s.cap, cams_dev, 1, ctx->cnt.as<uint32_t>(), ctx->acc.as<float4>(),
-                    ctx->rec.as<float4>(), ctx->gv.as<float4>(), s.grads.as<float4>(), accumulate ? 1 : 0, st);
+                    ctx->rec.as<float4>(), ctx->gcache.as<float4>(), ctx->gv.as<float4>(), s.grads.as<float4>(),
+                    accumulate ? 1 : 0, st);
     mark(ctx, 9);
     CK(cudaGetLastError());
     if (loss_out) {
@@ -701,7 +711,7 @@ void rgs_destroy(rgs_ctx* ctx) {
         s->params.release(); s->grads.release(); s->m1.release(); s->m2.release(); s->accum.release(); s->denom.release();
     }
     for (auto& t : ctx->targets) t.release();
-    DBuf* bufs[] = {&ctx->hdr, &ctx->outd, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->dkey, &ctx->ids, &ctx->acc, &ctx->gv, &ctx->pkeys, &ctx->pvals,
+    DBuf* bufs[] = {&ctx->hdr, &ctx->outd, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->gcache, &ctx->dkey, &ctx->ids, &ctx->acc, &ctx->gv, &ctx->pkeys, &ctx->pvals,
                     &ctx->ranges, &ctx->rgb, &ctx->final_t, &ctx->last, &ctx->dl, &ctx->partials, &ctx->scalars,
                     &ctx->block_sums, &ctx->view_pairs, &ctx->sort.hist, &ctx->sort.keys2, &ctx->sort.vals2, &ctx->dens_scratch,
                     &ctx->dens_out, &ctx->m_tmp, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->stage_d,
@@ -1369,10 +1379,11 @@ int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], fl
             a.skip_flag = (const int*)(sc + SC_OVERFLOW);
             a.bc_dev = hd->bc;
             launch_geometry_adam(cams_dev, V, s.n, s.cap, ctx->cnt.as<uint32_t>(), ctx->acc.as<float4>(),
-                                 ctx->rec.as<float4>(), ctx->gv.as<float4>(), a, st);
+                                 ctx->rec.as<float4>(), ctx->gcache.as<float4>(), ctx->gv.as<float4>(), a, st);
         } else {
             launch_geometry(s.params.as<float4>(), s.n, s.cap, cams_dev, V, ctx->cnt.as<uint32_t>(), ctx->acc.as<float4>(),
-                            ctx->rec.as<float4>(), ctx->gv.as<float4>(), s.grads.as<float4>(), accumulate, st);
+                            ctx->rec.as<float4>(), ctx->gcache.as<float4>(), ctx->gv.as<float4>(), s.grads.as<float4>(),
+                            accumulate, st);
         }
         mark(ctx, 9);
         cudaMemcpyAsync(&ctx->out_h->pairs, sc + SC_PAIRS, 4, cudaMemcpyDeviceToHost, st);
@@ -1420,6 +1431,7 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
     size_t S = (size_t)s.n * V;
     int rc = ensure_work(ctx, S, px_cap, tiles_cap, lb_cap, V);
     if (rc) return rc;
+    if ((rc = ensure_gcache(ctx, s))) return rc;
     if (!ctx->pkeys.p && (rc = ensure_pairs(ctx, S * 4))) return rc;
     if ((rc = ensure_moments(ctx, s, s.n))) return rc;
     if (host_targets) {
@@ -1443,7 +1455,7 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
         CK(cudaMemsetAsync(sc + SC_VISIBLE, 0, 4, ctx->st));
         launch_project(s.params.as<float4>(), s.n, s.cap, cams_dev, V, ctx->opt.tile_w, ctx->opt.tile_h, ctx->rec.as<float4>(),
                        ctx->cnt.as<uint32_t>(), ctx->tdesc.as<uint2>(), ctx->dkey.as<uint32_t>(), ctx->ids.as<uint32_t>(),
-                       zero_bg(bg) ? 1 : 0, sc + SC_VISIBLE, ctx->st);
+                       zero_bg(bg) ? 1 : 0, sc + SC_VISIBLE, ctx->gcache.as<float4>(), ctx->st);
         launch_view_pairs(ctx->cnt.as<uint32_t>(), (uint32_t)s.n, V, ctx->view_pairs.as<unsigned long long>(), ctx->st);
         CK(cudaGetLastError());
         unsigned long long per[MAX_VIEWS], total = 0;
@@ -1460,7 +1472,7 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
         h->bc[1] = 1.0f - powi_f(tc.beta2, (int)s.t);
         // Everything a captured graph bakes in: sizes, every buffer address, and
         // the loss weight, background and optimiser constants.
-        const DBuf* bufs[] = {&s.params, &s.grads, &s.m1, &s.m2, &s.accum, &s.denom, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->gv, &ctx->dkey,
+        const DBuf* bufs[] = {&s.params, &s.grads, &s.m1, &s.m2, &s.accum, &s.denom, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->gv, &ctx->gcache, &ctx->dkey,
                               &ctx->ids, &ctx->acc, &ctx->pkeys, &ctx->pvals, &ctx->ranges, &ctx->rgb, &ctx->final_t,
                               &ctx->last, &ctx->dl, &ctx->partials, &ctx->scalars, &ctx->block_sums, &ctx->hdr, &ctx->outd,
                               &ctx->sort.hist, &ctx->sort.keys2, &ctx->sort.vals2};
@@ -1987,6 +1999,7 @@ int debug_bin(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* 
     assign_bases(&dc, 1, px, tiles, lb);
     if ((rc = ensure_work(ctx, std::max<size_t>(n, 1), px, tiles, lb, 1))) return rc;
     if ((rc = upload_single_cam(ctx, dc, cams_dev))) return rc;
+    if ((rc = ensure_gcache(ctx, s))) return rc;
     return bin_batch(ctx, s, *cams_dev, 1, tiles, true, b);
 }
 

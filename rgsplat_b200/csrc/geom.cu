@@ -70,7 +70,8 @@ __device__ __forceinline__ float lane_of(const float4& v, int l) { return l == 0
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(128, 8) k_geom_view(const float4* __restrict__ params, int n, int cap, const DevCam* __restrict__ cams,
                                                    int nviews, const uint32_t* __restrict__ cnt, const float4* __restrict__ acc,
-                                                   const float4* __restrict__ rec, float4* __restrict__ gv) {
+                                                   const float4* __restrict__ rec, const float4* __restrict__ gcache,
+                                                   float4* __restrict__ gv) {
     const size_t S = (size_t)n * nviews;
     const size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S || cnt[s] == 0) return;
@@ -79,10 +80,11 @@ __global__ void __launch_bounds__(128, 8) k_geom_view(const float4* __restrict__
     const DevCam& c = cams[v];
     const float4 a0 = acc[s], a1 = acc[S + s], a2 = acc[2 * S + s];
     const float4 col = rec[2 * S + s];
-    const float4 p0 = params[i], p1 = params[(size_t)cap + i], p2 = params[2 * (size_t)cap + i];
+    const float4 p0 = params[i];
     const float pos[3] = {p0.x, p0.y, p0.z};
-    const float q[4] = {p1.x, p1.y, p1.z, p1.w};
-    const float sc[3] = {exp_cr(p2.x), exp_cr(p2.y), exp_cr(p2.z)};
+    // the 3D covariance of the projection (project.cu k_gauss_cache, this step)
+    const float4 g0 = gcache[i], g1 = gcache[(size_t)cap + i];
+    const M3 sig = {{{g0.y, g0.z, g0.w}, {g0.z, g1.x, g1.y}, {g0.w, g1.y, g1.z}}};
     float pc[3];
     cam_mul_g(c, pos, pc);
     const float fx = c.fx, fy = c.fy;
@@ -91,7 +93,6 @@ __global__ void __launch_bounds__(128, 8) k_geom_view(const float4* __restrict__
     for (int r = 0; r < 3; ++r)
 #pragma unroll
         for (int k = 0; k < 3; ++k) V.m[r][k] = c.view[r * 4 + k];
-    const M3 sig = build_cov3d(sc, q);
     // projection.rs:24-69 (the projection clamps tz; visible splats have tz > 0.001)
     const float tx = pc[0], ty = pc[1], tz = pc[2];
     const float tzc = fmaxf(tz, 0.001f);
@@ -372,24 +373,24 @@ __global__ void __launch_bounds__(128, 6) k_geom_gauss(const float4* __restrict_
 }
 
 static void launch_geom_view(const float4* params, int n, int cap, const DevCam* cams, int nviews, const uint32_t* cnt,
-                             const float4* acc, const float4* rec, float4* gv, cudaStream_t st) {
+                             const float4* acc, const float4* rec, const float4* gcache, float4* gv, cudaStream_t st) {
     size_t S = (size_t)n * nviews;
     if (S == 0) return;
-    k_geom_view<<<(unsigned)((S + 127) / 128), 128, 0, st>>>(params, n, cap, cams, nviews, cnt, acc, rec, gv);
+    k_geom_view<<<(unsigned)((S + 127) / 128), 128, 0, st>>>(params, n, cap, cams, nviews, cnt, acc, rec, gcache, gv);
 }
 
 void launch_geometry(const float4* params, int n, int cap, const DevCam* cams, int nviews, const uint32_t* cnt, const float4* acc,
-                     const float4* rec, float4* gv, float4* grads, int accumulate, cudaStream_t st) {
+                     const float4* rec, const float4* gcache, float4* gv, float4* grads, int accumulate, cudaStream_t st) {
     if (n <= 0) return;
-    launch_geom_view(params, n, cap, cams, nviews, cnt, acc, rec, gv, st);
+    launch_geom_view(params, n, cap, cams, nviews, cnt, acc, rec, gcache, gv, st);
     AdamArgs a{};
     k_geom_gauss<0><<<(n + 127) / 128, 128, 0, st>>>(params, n, cap, cams, nviews, cnt, gv, grads, accumulate, a);
 }
 
 void launch_geometry_adam(const DevCam* cams, int nviews, int n, int cap, const uint32_t* cnt, const float4* acc, const float4* rec,
-                          float4* gv, const AdamArgs& a, cudaStream_t st) {
+                          const float4* gcache, float4* gv, const AdamArgs& a, cudaStream_t st) {
     if (n <= 0) return;
-    launch_geom_view(a.params, n, cap, cams, nviews, cnt, acc, rec, gv, st);
+    launch_geom_view(a.params, n, cap, cams, nviews, cnt, acc, rec, gcache, gv, st);
     k_geom_gauss<1><<<(n + 127) / 128, 128, 0, st>>>(nullptr, n, cap, cams, nviews, cnt, gv, nullptr, 0, a);
 }
 

@@ -60,11 +60,48 @@ struct Projected {
     int box[4];
 };
 
-// backward.rs:210-280. Returns false when the Gaussian is culled.
+// The view-independent terms of a Gaussian's projection: sigmoid of the
+// opacity logit and the 3D covariance M M^T from exp(log-scales) and the
+// normalised quaternion. M M^T forms entry (i, j) and (j, i) from the same
+// products in the same order, so its six distinct entries hold it exactly.
+__device__ __forceinline__ M3 gauss_sigma(const float4* __restrict__ params, int cap, int i) {
+    const float4 p1 = params[(size_t)cap + i], p2 = params[2 * (size_t)cap + i];
+    const float q[4] = {p1.x, p1.y, p1.z, p1.w};
+    const float sc[3] = {exp_cr(p2.x), exp_cr(p2.y), exp_cr(p2.z)};
+    return build_cov3d(sc, q);
+}
+
+__device__ __forceinline__ M3 cached_sigma(const float4* __restrict__ gcache, int cap, int i) {
+    const float4 c0 = gcache[i], c1 = gcache[(size_t)cap + i];
+    return M3{{{c0.y, c0.z, c0.w}, {c0.z, c1.x, c1.y}, {c0.w, c1.y, c1.z}}};
+}
+
+// One thread per Gaussian, once per step: gcache[i] = (opacity, S00, S01,
+// S02), gcache[cap + i] = (S11, S12, S22, 0), so the per-view projection and
+// geometry read them instead of evaluating four exponentials and the
+// covariance once per view.
+__global__ void __launch_bounds__(256) k_gauss_cache(const float4* __restrict__ params, int n, int cap,
+                                                     float4* __restrict__ gcache) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float opacity = sigmoid(params[i].w);
+    const M3 sig = gauss_sigma(params, cap, i);
+    gcache[i] = make_float4(opacity, sig.m[0][0], sig.m[0][1], sig.m[0][2]);
+    gcache[(size_t)cap + i] = make_float4(sig.m[1][1], sig.m[1][2], sig.m[2][2], 0.0f);
+}
+
+void launch_gauss_cache(const float4* params, int n, int cap, float4* gcache, cudaStream_t st) {
+    if (n > 0) k_gauss_cache<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(params, n, cap, gcache);
+}
+
+// backward.rs:210-280. Returns false when the Gaussian is culled. With a
+// non-null gcache (k_gauss_cache of the same parameters) the opacity and the
+// 3D covariance are read from it.
 template <bool FULL>
-__device__ __forceinline__ bool project_one(const float4* __restrict__ params, int cap, int i, const DevCam& c, Projected& o) {
+__device__ __forceinline__ bool project_one(const float4* __restrict__ params, int cap, int i, const DevCam& c, Projected& o,
+                                            const float4* __restrict__ gcache = nullptr) {
     float4 p0 = params[i];
-    float opacity = sigmoid(p0.w);
+    float opacity = gcache ? gcache[i].x : sigmoid(p0.w);
     if (opacity < 1.0f / 255.0f) return false;
     float pos[3] = {p0.x, p0.y, p0.z};
     float pc[3];
@@ -75,11 +112,7 @@ __device__ __forceinline__ bool project_one(const float4* __restrict__ params, i
     float sy = c.fy * pc[1] / tz + c.cy;
     const float margin = 128.0f;
     if (sx < -margin || sx > (float)c.width + margin || sy < -margin || sy > (float)c.height + margin) return false;
-    float4 p1 = params[(size_t)cap + i];
-    float4 p2 = params[2 * (size_t)cap + i];
-    float q[4] = {p1.x, p1.y, p1.z, p1.w};
-    float sc[3] = {exp_cr(p2.x), exp_cr(p2.y), exp_cr(p2.z)};
-    M3 sig = build_cov3d(sc, q);
+    const M3 sig = gcache ? cached_sigma(gcache, cap, i) : gauss_sigma(params, cap, i);
     float abc[3];
     project_cov(sig, pc, c, abc);
     float a = abc[0], b = abc[1], cc = abc[2];
@@ -122,7 +155,8 @@ __global__ void __launch_bounds__(256, 5) k_project(const float4* __restrict__ p
                                                  const DevCam* __restrict__ cams, int nviews, int tile_w,
                                                  int tile_h, float4* __restrict__ rec, uint32_t* __restrict__ cnt,
                                                  uint2* __restrict__ tdesc, uint32_t* __restrict__ dkey,
-                                                 uint32_t* __restrict__ ids, int prune, uint32_t* __restrict__ visible) {
+                                                 uint32_t* __restrict__ ids, int prune, uint32_t* __restrict__ visible,
+                                                 const float4* __restrict__ gcache) {
     size_t S = (size_t)n * nviews;
     size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S) return;
@@ -131,7 +165,7 @@ __global__ void __launch_bounds__(256, 5) k_project(const float4* __restrict__ p
     const DevCam& c = cams[v];
     ids[s] = (uint32_t)s;
     Projected o;
-    if (!project_one<true>(params, cap, i, c, o)) {
+    if (!project_one<true>(params, cap, i, c, o, gcache)) {
         cnt[s] = 0;
         tdesc[s] = make_uint2(0u, 0u);
         dkey[s] = 0xFFFFFFFFu;
@@ -172,11 +206,13 @@ __global__ void __launch_bounds__(256, 5) k_project(const float4* __restrict__ p
 
 void launch_project(const float4* params, int n, int cap, const DevCam* cams, int nviews, int tile_w, int tile_h,
                     float4* rec, uint32_t* cnt, uint2* tdesc, uint32_t* dkey, uint32_t* ids, int prune, uint32_t* visible,
-                    cudaStream_t st) {
+                    float4* gcache, cudaStream_t st) {
     size_t S = (size_t)n * nviews;
     if (S == 0) return;
+    launch_gauss_cache(params, n, cap, gcache, st);
     unsigned blocks = (unsigned)((S + 255) / 256);
-    k_project<<<blocks, 256, 0, st>>>(params, n, cap, cams, nviews, tile_w, tile_h, rec, cnt, tdesc, dkey, ids, prune, visible);
+    k_project<<<blocks, 256, 0, st>>>(params, n, cap, cams, nviews, tile_w, tile_h, rec, cnt, tdesc, dkey, ids, prune, visible,
+                                      gcache);
 }
 
 // ---------------------------------------------------------------------------

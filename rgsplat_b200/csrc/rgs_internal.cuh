@@ -134,7 +134,11 @@ void launch_check_finite(const float4* planes, int n, int cap, int* flag, cudaSt
 // *visible (zeroed by the caller) gains the number of slots with cnt > 0.
 void launch_project(const float4* params, int n, int cap, const DevCam* cams, int nviews,
                     int tile_w, int tile_h, float4* rec, uint32_t* cnt, uint2* tdesc, uint32_t* dkey,
-                    uint32_t* ids, int prune, uint32_t* visible, cudaStream_t st);
+                    uint32_t* ids, int prune, uint32_t* visible, float4* gcache, cudaStream_t st);
+// Per-Gaussian view-independent projection terms ([2][cap] float4: opacity
+// and the 3D covariance's six entries), computed by launch_project first and
+// read by the geometry of the same step.
+void launch_gauss_cache(const float4* params, int n, int cap, float4* gcache, cudaStream_t st);
 void launch_project_wgsl(const float4* params, int n, int cap, const DevCam* cam, int cpu_math,
                          float* splats10, uint32_t* keys, cudaStream_t st);
 void launch_composite_prepare(const float* splats10, int n, const DevCam* cam, int tile_w, int tile_h,
@@ -247,10 +251,11 @@ struct AdamArgs {
 };
 // gv: per-slot scratch of 4 float4 planes (S = n * nviews slots).
 void launch_geometry(const float4* params, int n, int cap, const DevCam* cams, int nviews,
-                     const uint32_t* cnt, const float4* acc, const float4* rec, float4* gv, float4* grads,
-                     int accumulate, cudaStream_t st);
+                     const uint32_t* cnt, const float4* acc, const float4* rec, const float4* gcache, float4* gv,
+                     float4* grads, int accumulate, cudaStream_t st);
 void launch_geometry_adam(const DevCam* cams, int nviews, int n, int cap, const uint32_t* cnt,
-                          const float4* acc, const float4* rec, float4* gv, const AdamArgs& a, cudaStream_t st);
+                          const float4* acc, const float4* rec, const float4* gcache, float4* gv, const AdamArgs& a,
+                          cudaStream_t st);
 void launch_adam(int n, int cap, const float4* grads, const AdamArgs& a, cudaStream_t st);
 void launch_reset_opacities(float4* params, int n, int cap, cudaStream_t st);
 
