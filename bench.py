@@ -64,8 +64,8 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--tile", default="16x16")
-    p.add_argument("--batch", type=int, default=256)
-    p.add_argument("--ppt", type=int, default=2, help="pixels per thread of the blend kernels (1 or 2)")
+    p.add_argument("--batch", type=int, default=128)
+    p.add_argument("--ppt", type=int, default=2, help="pixels per thread of the forward blend (1 or 2; the backward takes twice as many)")
     p.add_argument("--no-autotune", action="store_true", help="keep --tile/--batch/--ppt instead of autotuning")
     p.add_argument("--no-variants", action="store_true", help="skip the recompute vs store-all backward measurement")
     p.add_argument("--no-rows", action="store_true", help="skip the preview / target / model-file row measurements")
@@ -627,12 +627,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             line["backward_variants"] = measure_backward_variants(R, scenes, local_rank)
         if not args.no_rows and world == 1:
             line["next_rows"] = measure_next_rows(R, g, cfg.cameras[0], local_rank, cpu=not args.no_cpu_baseline)
-        # kernels launched per batched step: project 1, depth sort 4x3, count
+        # kernels launched per batched step: term cache + project 2, depth sort 4x3, count
         # scan 2, emit 1, tile sort 3 per 8 bits, ranges 1, forward 1, loss 2,
         # backward 1, geometry+Adam 2 (+ memsets)
         ltw, lth = (int(x) for x in layout[0].split("x"))
         tile_bits = max(1, int(np.ceil(np.log2(max(2, V * max(-(-c.width // ltw) * -(-c.height // lth) for c in cfg.cameras))))))
-        per_step = 1 + 12 + 2 + 1 + 3 * ((tile_bits + 7) // 8) + 1 + 1 + 2 + 1 + 2
+        per_step = 2 + 12 + 2 + 1 + 3 * ((tile_bits + 7) // 8) + 1 + 1 + 2 + 1 + 2
         line["gpu_launches"] = per_step * args.steps
         print(json.dumps(line), flush=True)
     if dist is not None:
