@@ -120,15 +120,25 @@ __device__ __forceinline__ int stage_batch(const BlendArgs& a, size_t S, uint32_
 // Forward. PPT vertically adjacent pixels per thread share dx and the
 // dx-only products of power, which are evaluated once per (splat, thread) in
 // the reference's rounding order.
+// The TW threads that share a pixel row would each form dy and Q.z*dy*dy for
+// every splat; where the shared memory allows (ROWTERMS), the CTA forms them
+// once per (staged splat, tile row) after staging, with the same operations.
+template <int BATCH, int TH, int PPT>
+struct RowTerms {
+    static constexpr bool on = BATCH * TH <= 2048 && PPT == 2;
+};
+
 template <int TW, int TH, int BATCH, bool RECT, int PPT, bool STORE = false>
 __global__ void __launch_bounds__(TW * TH / PPT) k_blend_fwd(BlendArgs a) {
     constexpr int NT = TW * TH / PPT;
+    constexpr bool ROWTERMS = RowTerms<BATCH, TH, PPT>::on;
     __shared__ float4 s_a[BATCH];
     __shared__ float4 s_c[BATCH];
     __shared__ float4 s_k[BATCH];
     __shared__ int s_li[BATCH];
     __shared__ int s_wsum[NT / 32];
     __shared__ uint2 s_rall[RECT ? BATCH : 1];
+    __shared__ __align__(16) float2 s_row[ROWTERMS ? BATCH : 1][ROWTERMS ? TH : 1];  // (dy, Q.z*dy*dy)
     __shared__ int s_tile;
     constexpr int RW = (32 / TW) * PPT;  // pixel rows per warp
     const int tid = threadIdx.x;
@@ -181,18 +191,36 @@ __global__ void __launch_bounds__(TW * TH / PPT) k_blend_fwd(BlendArgs a) {
                     for (int j = 0; j < staged && !seen[p]; ++j)
                         if (in_rect(__uint_as_float(s_rall[j].x), __uint_as_float(s_rall[j].y), px, py0 + p)) seen[p] = true;
             }
+            if (ROWTERMS) {
+                for (int idx = tid; idx < nb * TH; idx += NT) {
+                    const int k = idx / TH, r = idx - k * TH;
+                    const float dy = ((float)(ty * TH + r) + 0.5f) - s_a[k].y;
+                    s_row[k][r] = make_float2(dy, s_c[k].z * dy * dy);
+                }
+                __syncthreads();
+            }
+            const int rbase = (tid / TW) * PPT;  // this thread's first row in the tile
             for (int k = 0; k < nb && !all_done; ++k) {
                 const float4 A = s_a[k];
                 const float4 Q = s_c[k];
                 const float dx = pxf - A.x;
                 const float tdx = Q.x * dx * dx;
                 const float t2b = 2.0f * Q.y * dx;
+                float4 rw = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                if (ROWTERMS) rw = *reinterpret_cast<const float4*>(&s_row[k][rbase]);
 #pragma unroll
                 for (int p = 0; p < PPT; ++p) {
                     if (done[p]) continue;
                     if (RECT && !in_rect(Q.w, s_k[k].w, px, py0 + p)) continue;
-                    const float dy = pyc[p] - A.y;
-                    const float power = -0.5f * (tdx + t2b * dy + Q.z * dy * dy);
+                    float dy, qdd;
+                    if (ROWTERMS) {
+                        dy = p == 0 ? rw.x : rw.z;
+                        qdd = p == 0 ? rw.y : rw.w;
+                    } else {
+                        dy = pyc[p] - A.y;
+                        qdd = Q.z * dy * dy;
+                    }
+                    const float power = -0.5f * (tdx + t2b * dy + qdd);
                     if (power > 0.0f || power < A.w) continue;
                     const float alpha = fminf(A.z * expf_fast_nonpos(power), 0.99f);
                     if (alpha < 1.0f / 255.0f) continue;
