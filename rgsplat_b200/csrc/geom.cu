@@ -73,10 +73,13 @@ __global__ void __launch_bounds__(128, 8) k_geom_view(const float4* __restrict__
                                                    const float4* __restrict__ rec, const float4* __restrict__ gcache,
                                                    float4* __restrict__ gv) {
     const size_t S = (size_t)n * nviews;
-    const size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= S || cnt[s] == 0) return;
-    const int v = (int)(s / (size_t)n);
-    const int i = (int)(s - (size_t)v * n);
+    // chunk-major grid (as k_project): the per-Gaussian reads of the nviews
+    // consecutive blocks are shared through L2
+    const int v = (int)(blockIdx.x % (unsigned)nviews);
+    const int i = (int)((blockIdx.x / (unsigned)nviews) * blockDim.x + threadIdx.x);
+    if (i >= n) return;
+    const size_t s = (size_t)v * n + i;
+    if (cnt[s] == 0) return;
     const DevCam& c = cams[v];
     const float4 a0 = acc[s], a1 = acc[S + s], a2 = acc[2 * S + s];
     const float4 col = rec[2 * S + s];
@@ -376,7 +379,7 @@ static void launch_geom_view(const float4* params, int n, int cap, const DevCam*
                              const float4* acc, const float4* rec, const float4* gcache, float4* gv, cudaStream_t st) {
     size_t S = (size_t)n * nviews;
     if (S == 0) return;
-    k_geom_view<<<(unsigned)((S + 127) / 128), 128, 0, st>>>(params, n, cap, cams, nviews, cnt, acc, rec, gcache, gv);
+    k_geom_view<<<(unsigned)(((size_t)n + 127) / 128 * (size_t)nviews), 128, 0, st>>>(params, n, cap, cams, nviews, cnt, acc, rec, gcache, gv);
 }
 
 void launch_geometry(const float4* params, int n, int cap, const DevCam* cams, int nviews, const uint32_t* cnt, const float4* acc,

@@ -157,11 +157,14 @@ __global__ void __launch_bounds__(256, 5) k_project(const float4* __restrict__ p
                                                  uint2* __restrict__ tdesc, uint32_t* __restrict__ dkey,
                                                  uint32_t* __restrict__ ids, int prune, uint32_t* __restrict__ visible,
                                                  const float4* __restrict__ gcache) {
-    size_t S = (size_t)n * nviews;
-    size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= S) return;
-    int v = (int)(s / (size_t)n);
-    int i = (int)(s - (size_t)v * n);
+    // chunk-major grid: the nviews consecutive blocks project the same 256
+    // Gaussians into every view, so the per-Gaussian reads (SH, position,
+    // cached terms) of all but the first view come from L2
+    const size_t S = (size_t)n * nviews;
+    const int v = (int)(blockIdx.x % (unsigned)nviews);
+    const int i = (int)((blockIdx.x / (unsigned)nviews) * blockDim.x + threadIdx.x);
+    if (i >= n) return;
+    const size_t s = (size_t)v * n + i;
     const DevCam& c = cams[v];
     ids[s] = (uint32_t)s;
     Projected o;
@@ -210,7 +213,7 @@ void launch_project(const float4* params, int n, int cap, const DevCam* cams, in
     size_t S = (size_t)n * nviews;
     if (S == 0) return;
     launch_gauss_cache(params, n, cap, gcache, st);
-    unsigned blocks = (unsigned)((S + 255) / 256);
+    unsigned blocks = (unsigned)(((size_t)n + 255) / 256 * (size_t)nviews);
     k_project<<<blocks, 256, 0, st>>>(params, n, cap, cams, nviews, tile_w, tile_h, rec, cnt, tdesc, dkey, ids, prune, visible,
                                       gcache);
 }
