@@ -349,7 +349,32 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit_pruned(const uint32_t* __r
                 const uint32_t gtot = __shfl_sync(0xffffffffu, incl, EG - 1, EG);
                 uint32_t p = written + incl - span;
                 const uint32_t key0 = tbase + (uint32_t)((ty0 + row) * tiles_x + c0);
-                for (uint32_t t = 0; t < span; ++t, ++p) {
+                // two entries per 8-byte store once the output index is even
+                // (pk, pv hold the run that starts at entry out0)
+                uint32_t t = 0;
+                if (((out0 + p) & 1ull) && t < span) {
+                    if (p < room) {
+                        pk[p] = key0;
+                        pv[p] = slot;
+                    } else {
+                        *overflow = 1;
+                    }
+                    ++t;
+                    ++p;
+                }
+                for (; t + 1 < span; t += 2, p += 2) {
+                    if (p + 1 < room) {
+                        *reinterpret_cast<uint2*>(pk + p) = make_uint2(key0 + t, key0 + t + 1);
+                        *reinterpret_cast<uint2*>(pv + p) = make_uint2(slot, slot);
+                    } else {
+                        if (p < room) {
+                            pk[p] = key0 + t;
+                            pv[p] = slot;
+                        }
+                        *overflow = 1;
+                    }
+                }
+                if (t < span) {
                     if (p < room) {
                         pk[p] = key0 + t;
                         pv[p] = slot;
