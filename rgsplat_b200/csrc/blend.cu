@@ -125,7 +125,7 @@ __device__ __forceinline__ int stage_batch(const BlendArgs& a, size_t S, uint32_
 // once per (staged splat, tile row) after staging, with the same operations.
 template <int BATCH, int TH, int PPT>
 struct RowTerms {
-    static constexpr bool on = BATCH * TH <= 2048 && PPT == 2;
+    static constexpr bool on = BATCH * TH <= 2048 && PPT % 2 == 0;
 };
 
 template <int TW, int TH, int BATCH, bool RECT, int PPT, bool STORE = false>
@@ -206,16 +206,18 @@ __global__ void __launch_bounds__(TW * TH / PPT) k_blend_fwd(BlendArgs a) {
                 const float dx = pxf - A.x;
                 const float tdx = Q.x * dx * dx;
                 const float t2b = 2.0f * Q.y * dx;
-                float4 rw = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                if (ROWTERMS) rw = *reinterpret_cast<const float4*>(&s_row[k][rbase]);
+                float4 rw[(PPT + 1) / 2];  // two rows' (dy, Q.z*dy*dy) per 16-byte load
+#pragma unroll
+                for (int h = 0; h < (PPT + 1) / 2; ++h)
+                    rw[h] = ROWTERMS ? *reinterpret_cast<const float4*>(&s_row[k][rbase + 2 * h]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 #pragma unroll
                 for (int p = 0; p < PPT; ++p) {
                     if (done[p]) continue;
                     if (RECT && !in_rect(Q.w, s_k[k].w, px, py0 + p)) continue;
                     float dy, qdd;
                     if (ROWTERMS) {
-                        dy = p == 0 ? rw.x : rw.z;
-                        qdd = p == 0 ? rw.y : rw.w;
+                        dy = (p & 1) ? rw[p >> 1].z : rw[p >> 1].x;
+                        qdd = (p & 1) ? rw[p >> 1].w : rw[p >> 1].y;
                     } else {
                         dy = pyc[p] - A.y;
                         qdd = Q.z * dy * dy;
