@@ -634,10 +634,10 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             line["next_rows"] = measure_next_rows(R, g, cfg.cameras[0], local_rank, cpu=not args.no_cpu_baseline)
         # kernels launched per batched step: term cache + project 2, depth sort 4x3, count
         # scan 2, emit 1, tile sort 3 per 8 bits, ranges 1, forward 1, loss 2,
-        # backward 1, geometry+Adam 2 (+ memsets)
+        # backward 1, geometry+Adam 3 (per view, SH half, geometry half) (+ memsets)
         ltw, lth = (int(x) for x in layout[0].split("x"))
         tile_bits = max(1, int(np.ceil(np.log2(max(2, V * max(-(-c.width // ltw) * -(-c.height // lth) for c in cfg.cameras))))))
-        per_step = 2 + 12 + 2 + 1 + 3 * ((tile_bits + 7) // 8) + 1 + 1 + 2 + 1 + 2
+        per_step = 2 + 12 + 2 + 1 + 3 * ((tile_bits + 7) // 8) + 1 + 1 + 2 + 1 + 3
         line["gpu_launches"] = per_step * args.steps
         print(json.dumps(line), flush=True)
     if dist is not None:

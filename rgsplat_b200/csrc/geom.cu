@@ -244,9 +244,13 @@ __device__ __forceinline__ float4 adam_plane(int p, int i, int cap, float4 pv, f
 }
 
 // (B) per Gaussian. MODE 0: write the gradient planes (accumulate if asked);
-// MODE 1: apply Adam.
-template <int MODE>
-__global__ void __launch_bounds__(128, 6) k_geom_gauss(const float4* __restrict__ params_in, int n, int cap,
+// MODE 1: apply Adam. PART 0 does both halves; PART 1 only the SH planes
+// (3..14) and PART 2 only the geometry planes (0..2) with grad_accum/denom,
+// each with fewer registers, so more warps per SM hide the memory latency.
+// PART 1 must run before PART 2: it reads the position that PART 2's Adam
+// step rewrites.
+template <int MODE, int PART = 0>
+__global__ void __launch_bounds__(128, PART == 2 ? 8 : 6) k_geom_gauss(const float4* __restrict__ params_in, int n, int cap,
                                                     const DevCam* __restrict__ cams, int nviews, const uint32_t* __restrict__ cnt,
                                                     const float4* __restrict__ gv, float4* __restrict__ grads, int accumulate,
                                                     AdamArgs a) {
@@ -262,6 +266,7 @@ __global__ void __launch_bounds__(128, 6) k_geom_gauss(const float4* __restrict_
     const float4* params = MODE == 1 ? a.params : params_in;
     const float4 p0 = params[i];
     const float pos[3] = {p0.x, p0.y, p0.z};
+    if (PART != 2) {
     // ---- SH planes: sum_v mask_v[ch] * basis_v (the basis once per view, all
     // 48 sums in registers), then Adam / store per plane
     float shg[3][16];
@@ -301,6 +306,8 @@ __global__ void __launch_bounds__(128, 6) k_geom_gauss(const float4* __restrict_
             }
         }
     }
+    }
+    if (PART == 1) return;
     // ---- geometry: sums over views
     float dpos[3] = {0.0f, 0.0f, 0.0f}, dop = 0.0f, dS[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, screen = 0.0f;
     for (int v = 0; v < nviews; ++v) {
@@ -394,7 +401,8 @@ void launch_geometry_adam(const DevCam* cams, int nviews, int n, int cap, const 
                           const float4* gcache, float4* gv, const AdamArgs& a, cudaStream_t st) {
     if (n <= 0) return;
     launch_geom_view(a.params, n, cap, cams, nviews, cnt, acc, rec, gcache, gv, st);
-    k_geom_gauss<1><<<(n + 127) / 128, 128, 0, st>>>(nullptr, n, cap, cams, nviews, cnt, gv, nullptr, 0, a);
+    k_geom_gauss<1, 1><<<(n + 127) / 128, 128, 0, st>>>(nullptr, n, cap, cams, nviews, cnt, gv, nullptr, 0, a);
+    k_geom_gauss<1, 2><<<(n + 127) / 128, 128, 0, st>>>(nullptr, n, cap, cams, nviews, cnt, gv, nullptr, 0, a);
 }
 
 __global__ void __launch_bounds__(256) k_adam(int n, int cap, const float4* __restrict__ grads, AdamArgs a) {
