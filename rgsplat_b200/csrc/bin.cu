@@ -27,16 +27,7 @@ constexpr int EMIT_VT = 8;     // consecutive pairs per thread per emit round
 // words hits 32 distinct banks
 __device__ __forceinline__ int emit_pad(int i) { return i + (i >> 5); }
 
-int bin_grid_blocks() {
-    static int g = 0;
-    if (!g) {
-        int dev = 0, sms = 148;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        g = sms * 6;
-    }
-    return g;
-}
+int bin_grid_blocks() { return device_sm_count() * 6; }
 
 __device__ __forceinline__ void bin_chunk(uint32_t n, int G, int b, uint32_t& begin, uint32_t& end) {
     uint32_t chunk = (uint32_t)(((uint64_t)n + G - 1) / G);

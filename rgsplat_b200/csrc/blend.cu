@@ -509,19 +509,26 @@ static BlendKernel select_kernel(int tw, int th, int batch, bool rect, bool fwd,
     return rect ? pick_batch<16, 16, true>(batch, fwd, ppt) : pick_batch<16, 16, false>(batch, fwd, ppt);
 }
 
+// Persistent grid of a blend kernel on the current device: SMs x resident CTAs,
+// cached per (kernel, device ordinal).
 static int grid_for(BlendKernel k, int threads) {
+    struct Entry { BlendKernel k; int dev; int grid; };
     static std::mutex mu;
-    static std::pair<BlendKernel, int> cache[128];
+    static Entry cache[256];
     static int ncache = 0;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) cudaGetLastError();
+    const int sms = device_sm_count();
     std::lock_guard<std::mutex> g(mu);
     for (int i = 0; i < ncache; ++i)
-        if (cache[i].first == k) return cache[i].second;
-    int dev = 0, sms = 148, per = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k, threads, 0);
+        if (cache[i].k == k && cache[i].dev == dev) return cache[i].grid;
+    int per = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k, threads, 0) != cudaSuccess) {
+        cudaGetLastError();
+        per = 1;
+    }
     int grid = sms * std::max(per, 1);
-    if (ncache < 128) cache[ncache++] = {k, grid};
+    if (ncache < 256) cache[ncache++] = {k, dev, grid};
     return grid;
 }
 

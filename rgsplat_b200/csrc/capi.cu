@@ -575,8 +575,8 @@ int run_view_plain(rgs_ctx* ctx, Scene& s, const DevCam& dc_in, const float* tar
     }
     if (!do_backward) return RGS_OK;
     float* losses_dev = (float*)((char*)ctx->outd.p + offsetof(StepOut, losses));
-    launch_loss(cams_dev, 1, (int)lb, ctx->rgb.as<float>(), lambda, ctx->dl.as<float>(), ctx->partials.as<float>(), losses_dev,
-                nullptr, st);
+    CK(launch_loss(cams_dev, 1, (int)lb, ctx->rgb.as<float>(), lambda, ctx->dl.as<float>(), ctx->partials.as<float>(),
+                   losses_dev, nullptr, st));
     mark(ctx, 7);
     CK(cudaMemsetAsync(ctx->acc.p, 0, std::max<size_t>(s.n, 1) * 3 * sizeof(float4), st));
     BlendArgs ba = blend_args(ctx, s, cams_dev, 1, nullptr, tiles, b, bg, false);
@@ -680,6 +680,9 @@ int rgs_create(const rgs_options* opts, rgs_ctx** out) {
     ctx->device = o.device;
     cudaError_t e = cudaSetDevice(o.device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, o.device);
+    // one-time per-device kernel attributes, set here so that no later call
+    // (possibly inside a stream capture) has to
+    if (e == cudaSuccess) e = prepare_loss_kernel();
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
     ctx->st = ctx->own_stream;
     if (e == cudaSuccess) e = cudaMallocHost((void**)&ctx->hdr_h, sizeof(StepHdr));
@@ -923,8 +926,8 @@ int rgs_photometric_loss_grad(rgs_ctx* ctx, const float* rendered_rgb, const flo
     DevCam* cams_dev;
     if ((rc = upload_single_cam(ctx, dc, &cams_dev))) return rc;
     float* losses_dev = (float*)((char*)ctx->outd.p + offsetof(StepOut, losses));
-    launch_loss(cams_dev, 1, (int)lb, ctx->rgb.as<float>(), lambda, ctx->dl.as<float>(), ctx->partials.as<float>(), losses_dev,
-                nullptr, ctx->st);
+    CK(launch_loss(cams_dev, 1, (int)lb, ctx->rgb.as<float>(), lambda, ctx->dl.as<float>(), ctx->partials.as<float>(),
+                   losses_dev, nullptr, ctx->st));
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(loss_out, losses_dev, 4, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemcpyAsync(dl_out, ctx->dl.p, px * 12, cudaMemcpyDeviceToHost, ctx->st));
@@ -1365,8 +1368,9 @@ int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], fl
         // the step's targets were copied from host memory on copy_st, issued
         // just before this graph's launch; only the loss waits for them
         if (host_targets) cudaStreamWaitEvent(st, ctx->ev_copy, cudaEventWaitExternal);
-        launch_loss(cams_dev, V, 0, ctx->rgb.as<float>(), lambda, ctx->dl.as<float>(), ctx->partials.as<float>(), losses_dev,
-                    &hd->total_loss_blocks, st);
+        cudaError_t le = launch_loss(cams_dev, V, 0, ctx->rgb.as<float>(), lambda, ctx->dl.as<float>(),
+                                     ctx->partials.as<float>(), losses_dev, &hd->total_loss_blocks, st);
+        if (le != cudaSuccess) rc = cuda_fail(ctx, le, "loss kernel launch");
         mark(ctx, 7);
         cudaMemsetAsync(ctx->acc.p, 0, std::max<size_t>(S, 1) * 3 * sizeof(float4), st);
         BlendArgs ba = blend_args(ctx, s, cams_dev, V, &hd->total_tiles, tiles_cap, b, bg, false);
@@ -2113,8 +2117,8 @@ int rgs_debug_backward(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs
     BlendArgs fa = blend_args(ctx, ctx->sc, cams_dev, 1, nullptr, tiles, b, bg, true);
     launch_blend_forward(fa, ctx->opt.tile_w, ctx->opt.tile_h, ctx->opt.batch, ctx->st);
     float* losses_dev = (float*)((char*)ctx->outd.p + offsetof(StepOut, losses));
-    launch_loss(cams_dev, 1, (int)lb, ctx->rgb.as<float>(), lambda, ctx->dl.as<float>(), ctx->partials.as<float>(), losses_dev,
-                nullptr, ctx->st);
+    CK(launch_loss(cams_dev, 1, (int)lb, ctx->rgb.as<float>(), lambda, ctx->dl.as<float>(), ctx->partials.as<float>(),
+                   losses_dev, nullptr, ctx->st));
     CK(cudaMemsetAsync(ctx->acc.p, 0, std::max<size_t>(n, 1) * 3 * sizeof(float4), ctx->st));
     BlendArgs ba = blend_args(ctx, ctx->sc, cams_dev, 1, nullptr, tiles, b, bg, false);
     launch_blend_backward(ba, ctx->opt.tile_w, ctx->opt.tile_h, ctx->opt.batch, ctx->st);

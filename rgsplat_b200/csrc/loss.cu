@@ -16,6 +16,8 @@
 // formed once per run) and accumulate with FMA; the SSIM map arithmetic
 // keeps the reference's expressions. The scalar loss is reduced per CTA and
 // then per view in a fixed order (deterministic).
+#include <mutex>
+
 #include "rgs_internal.cuh"
 #include "rgs_math.cuh"
 
@@ -300,20 +302,30 @@ __global__ void __launch_bounds__(FIN_THREADS) k_loss_finalize(const DevCam* __r
     }
 }
 
-void launch_loss(const DevCam* cams, int nviews, int total_blocks, const float* rgb, float lambda, float* dl, float* partials,
-                 float* losses, const uint32_t* total_dev, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_loss, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LOSS_SMEM);
-        attr = true;
-    }
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+cudaError_t prepare_loss_kernel() {
+    static std::mutex mu;
+    static bool ready[64];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
+    if (ready[dev]) return cudaSuccess;
+    e = cudaFuncSetAttribute(k_loss, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LOSS_SMEM);
+    if (e == cudaSuccess) ready[dev] = true;
+    return e;
+}
+
+cudaError_t launch_loss(const DevCam* cams, int nviews, int total_blocks, const float* rgb, float lambda, float* dl,
+                        float* partials, float* losses, const uint32_t* total_dev, cudaStream_t st) {
+    cudaError_t e = prepare_loss_kernel();
+    if (e != cudaSuccess) return e;
+    const int sms = device_sm_count();
     int grid = total_dev ? sms * 2 : (total_blocks < sms * 2 ? total_blocks : sms * 2);
     if (grid < 1) grid = 1;
     k_loss<<<grid, LOSS_THREADS, LOSS_SMEM, st>>>(cams, nviews, total_dev, total_blocks, rgb, lambda, dl, partials);
     if (nviews > 0) k_loss_finalize<<<nviews, FIN_THREADS, 0, st>>>(cams, nviews, partials, lambda, losses);
+    return cudaGetLastError();
 }
 
 }  // namespace rgs

@@ -102,6 +102,9 @@ extern "C" int rgs_photometric_loss_grad_noalloc(int device, const float* render
         if (!g_na_ptr[device]) {
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            // the loss kernel's shared-memory limit, set on this device now
+            // rather than on a later call that may be inside a stream capture
+            if (e == cudaSuccess) e = prepare_loss_kernel();
             if (e != cudaSuccess) rc = cuda_err(err, err_len, e);
             else g_na_ptr[device] = p;
         }
@@ -117,8 +120,9 @@ extern "C" int rgs_photometric_loss_grad_noalloc(int device, const float* render
         float* partials = (float*)(scratch + NA_HEADER);
         cudaStream_t st = (cudaStream_t)cuda_stream;
         k_noalloc_put_cam<<<1, 1, 0, st>>>(c, cam_dev);
-        launch_loss(cam_dev, 1, (int)blocks, rendered_rgb, lambda, dl_out, partials, loss_out, nullptr, st);
-        if ((e = cudaGetLastError()) != cudaSuccess) rc = cuda_err(err, err_len, e);
+        if ((e = cudaGetLastError()) == cudaSuccess)
+            e = launch_loss(cam_dev, 1, (int)blocks, rendered_rgb, lambda, dl_out, partials, loss_out, nullptr, st);
+        if (e != cudaSuccess) rc = cuda_err(err, err_len, e);
     }
     cudaSetDevice(prev);
     return rc;

@@ -120,6 +120,9 @@ struct SfmScratch {
 
 // ---- launchers (each defined in the .cu file named in the comment) --------
 
+// device.cu: SM count of the current device, cached per device ordinal.
+int device_sm_count();
+
 // layout.cu
 void launch_aos_to_planes(const float* aos, float4* planes, int n, int cap, cudaStream_t st);
 void launch_planes_to_aos(const float4* planes, float* aos, int n, int cap, cudaStream_t st);
@@ -231,9 +234,14 @@ void launch_unpack_ply(const uint8_t* body, size_t stride, int n, const PlyField
                        float4* params, int cap, cudaStream_t st);
 
 // loss.cu
-void launch_loss(const DevCam* cams, int nviews, int total_blocks, const float* rgb, float lambda,
-                 float* dl, float* partials, float* losses, const uint32_t* total_dev,
-                 cudaStream_t st);
+// The loss kernel needs more dynamic shared memory than the default limit; the
+// limit is a per-device function attribute, set on the current device the
+// first time this is called there (under a mutex; later calls return at once).
+cudaError_t prepare_loss_kernel();
+// Prepares the current device (above), then enqueues the loss kernels.
+cudaError_t launch_loss(const DevCam* cams, int nviews, int total_blocks, const float* rgb, float lambda,
+                        float* dl, float* partials, float* losses, const uint32_t* total_dev,
+                        cudaStream_t st);
 
 // geom.cu
 struct AdamArgs {

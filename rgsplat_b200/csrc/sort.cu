@@ -325,16 +325,7 @@ __global__ void __launch_bounds__(SORT_THREADS) k_downsweep(const uint32_t* __re
     }
 }
 
-int sort_grid_blocks() {
-    static int g = 0;
-    if (!g) {
-        int dev = 0, sms = 148;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        g = sms * 4;
-    }
-    return g;
-}
+int sort_grid_blocks() { return device_sm_count() * 4; }
 
 int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n_host, const uint32_t* n_dev, int bits, SortScratch& sc,
                      int grid, cudaStream_t st, cudaError_t* err) {

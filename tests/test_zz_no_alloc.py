@@ -24,15 +24,15 @@ def _images(seed, w, h):
     return rendered, target
 
 
-def _noalloc(lib, torch, rendered, target, w, h, lam):
-    dev = torch.device("cuda:0")
+def _noalloc(lib, torch, rendered, target, w, h, lam, device=0):
+    dev = torch.device(f"cuda:{device}")
     r = torch.from_numpy(rendered).to(dev)
     t = torch.from_numpy(target).to(dev)
     dl = torch.full((w * h * 3,), float("nan"), device=dev)
     loss = torch.full((1,), float("nan"), device=dev)
     err = C.create_string_buffer(256)
     stream = torch.cuda.current_stream(dev)
-    rc = lib.rgs_photometric_loss_grad_noalloc(0, r.data_ptr(), t.data_ptr(), w, h, lam, loss.data_ptr(),
+    rc = lib.rgs_photometric_loss_grad_noalloc(device, r.data_ptr(), t.data_ptr(), w, h, lam, loss.data_ptr(),
                                                dl.data_ptr(), stream.cuda_stream, err, len(err))
     assert rc == 0, err.value.decode()
     stream.synchronize()
@@ -55,6 +55,26 @@ def test_noalloc_matches_context_entry_point_twice():
         assert np.isfinite(got_loss) and np.all(np.isfinite(got_dl))
         assert np.float32(got_loss) == np.float32(want_loss)
         assert np.array_equal(got_dl, want_dl)
+
+
+def test_noalloc_on_a_second_device():
+    """The first call on each device sets that device up (scratch address and
+    the loss kernel's shared-memory limit): a call on device 1 after device 0,
+    before any context exists on device 1, must match the context entry point
+    there. Needs two GPUs; skipped otherwise."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available() or torch.cuda.device_count() < 2:
+        pytest.skip("needs two GPUs")
+    from rgsplat_b200 import _lib, api
+
+    lib = _lib.load()
+    w, h, lam = 257, 130, 0.2
+    rendered, target = _images(13, w, h)
+    got = [_noalloc(lib, torch, rendered, target, w, h, lam, device=d) for d in (0, 1)]
+    for d in (0, 1):
+        want_loss, want_dl = api.photometric_loss_grad(rendered, target, w, h, lam, ctx=api.Context(device=d))
+        assert np.float32(got[d][0]) == np.float32(want_loss)
+        assert np.array_equal(got[d][1], want_dl)
 
 
 def test_noalloc_rejects_images_beyond_scratch():
