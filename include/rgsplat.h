@@ -210,8 +210,9 @@ int rgs_adam_step(rgs_ctx* ctx, float* gaussians, size_t n, const float* grads, 
                   const rgs_train_config* cfg);
 
 /* pipeline::optimizer::densify_and_prune (src/pipeline/optimizer.rs:206-272).
- * Writes the new Gaussians to out (capacity out_cap Gaussians; 3*n always
- * suffices) and their count to *n_out. Returns RGS_ERR_CAPACITY with *n_out
+ * Writes the new Gaussians to out (capacity out_cap Gaussians; 2*n always
+ * suffices: every Gaussian is kept and cloned at most, or split into two)
+ * and their count to *n_out. Returns RGS_ERR_CAPACITY with *n_out
  * set to the required count when out_cap is too small. As AdamState::resize
  * does, the caller grows its moment arrays to *n_out if larger (never
  * shrinking them) and zeroes grad_accum / grad_denom. */
@@ -353,6 +354,25 @@ typedef struct rgs_stats {
     uint32_t reserved;
 } rgs_stats;
 int rgs_get_stats(rgs_ctx* ctx, rgs_stats* out);
+
+/* Device memory the context holds through its own buffers (parameters,
+ * moments, targets, per-step work and pair buffers, sort scratch), and the
+ * most it has held since it was created or since the last call with
+ * reset_peak != 0 (which then restarts the high-water mark at the bytes held).
+ * Either pointer may be NULL. The reference keeps no device state; this is
+ * how the recompute and store-all backward variants report peak memory. */
+int rgs_get_memory(rgs_ctx* ctx, uint64_t* held_bytes, uint64_t* peak_bytes, int reset_peak);
+
+/* (pixel, splat) pairs the blend kernels evaluated in the trainer's most
+ * recent batched pass (run as one view group): the forward walks each pixel's
+ * tile list until the transmittance drops below 1e-4 (ending at the last
+ * contributor) or the list ends, the backward walks from the last contributor
+ * to the front (forward_pass / backward_pass, src/cpu/backward.rs:296-512).
+ * The lists are the ones the pass blended (pruned to each row's reachable span
+ * when the background is zero). The reference has no such counter: it is the
+ * work measure of the blend kernels' FP32 roofline. RGS_ERR_INVALID_ARG when
+ * no batched pass holds the pixel buffers. */
+int rgs_trainer_evaluated_pairs(rgs_ctx* ctx, uint64_t* forward_pairs, uint64_t* backward_pairs);
 
 /* ---- tiling and its autotuner ---------------------------------------------
  * Tile shape, splats staged per batch and pixels per thread change only how

@@ -39,6 +39,17 @@ int rgs_debug_forward(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_
 int rgs_debug_backward(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, const float* target_rgba,
                        const float bg[3], float lambda, float* acc9, float* dl_dpix);
 
+/* Pixels of the view at position k of the trainer's most recent batched pass
+ * (rgs_trainer_step or rgs_trainer_backward with RGS_STEP_BATCHED that ran as
+ * one view group), read from the batch's own buffers: rgb w*h*3, final T w*h
+ * and dL/dpixel w*h*3, each may be NULL. This is forward_pass's output and
+ * photometric_loss_grad's gradient (backward.rs:296-385, 646-693) for every
+ * view of a batch, for comparison with per-view reference renders.
+ * RGS_ERR_INVALID_ARG when no such pass holds the buffers (another call has
+ * written them since, or the batch ran as several view groups) or k is out of
+ * range. */
+int rgs_debug_trainer_batch_pixels(rgs_ctx* ctx, size_t k, float* rgb, float* final_t, float* dl_dpix);
+
 #ifdef __cplusplus
 }
 #endif

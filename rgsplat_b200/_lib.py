@@ -203,6 +203,8 @@ SIGNATURES = {
     "rgs_trainer_reset_opacities": (C.c_int, [CTX]),
     "rgs_trainer_get_adam_state": (C.c_int, [CTX, C.POINTER(rgs_adam_state)]),
     "rgs_trainer_set_adam_state": (C.c_int, [CTX, C.POINTER(rgs_adam_state)]),
+    "rgs_get_memory": (C.c_int, [CTX, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_int]),
+    "rgs_trainer_evaluated_pairs": (C.c_int, [CTX, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "rgs_get_stats": (C.c_int, [CTX, C.POINTER(rgs_stats)]),
     "rgs_get_options": (C.c_int, [CTX, C.POINTER(rgs_options)]),
     "rgs_set_tiling": (C.c_int, [CTX, C.c_int, C.c_int, C.c_int, C.c_int]),
@@ -217,6 +219,7 @@ SIGNATURES = {
                                        C.POINTER(C.c_int32), C.c_size_t]),
     "rgs_debug_forward": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), FP, FP, FP, C.POINTER(C.c_int32)]),
     "rgs_debug_backward": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), FP, FP, C.c_float, FP, FP]),
+    "rgs_debug_trainer_batch_pixels": (C.c_int, [CTX, C.c_size_t, FP, FP, FP]),
 }
 
 

@@ -159,6 +159,7 @@ class Context:
             raise RgsError(rc, "rgs_create failed")
         self.handle = h
         self.create_options = o
+        self.stream = None  # cudaStream_t the context issues on; None: its own
 
     def check(self, rc: int) -> None:
         if rc != L.RGS_OK:
@@ -179,6 +180,7 @@ class Context:
     def set_stream(self, cuda_stream: int | None) -> None:
         """Issue work on an external cudaStream_t (not the legacy default stream)."""
         self.check(self.lib.rgs_set_stream(self.handle, C.c_void_p(cuda_stream or None)))
+        self.stream = int(cuda_stream) if cuda_stream else None
 
     def set_profiling(self, on: bool) -> None:
         self.check(self.lib.rgs_set_profiling(self.handle, 1 if on else 0))
@@ -193,6 +195,14 @@ class Context:
         s = L.rgs_stats()
         self.check(self.lib.rgs_get_stats(self.handle, C.byref(s)))
         return {name: getattr(s, name) for name, _ in L.rgs_stats._fields_}
+
+    def memory(self, reset_peak: bool = False) -> dict:
+        """Device bytes this context holds through its own buffers and the most
+        it has held since creation or the last reset_peak (which restarts the
+        high-water mark at the bytes held)."""
+        held, peak = C.c_uint64(0), C.c_uint64(0)
+        self.check(self.lib.rgs_get_memory(self.handle, C.byref(held), C.byref(peak), 1 if reset_peak else 0))
+        return {"held_bytes": int(held.value), "peak_bytes": int(peak.value)}
 
     def options(self) -> dict:
         o = L.rgs_options()
@@ -418,7 +428,7 @@ def densify_and_prune(gaussians, state: AdamState, cfg: TrainConfig, scene_exten
     ctx = ctx or default_context()
     g = _gauss(gaussians)
     n = g.shape[0]
-    out = np.zeros((3 * n + 1, GAUSSIAN_FLOATS), np.float32)
+    out = np.zeros((2 * n + 1, GAUSSIAN_FLOATS), np.float32)  # kept + cloned, or split in two
     n_out = C.c_size_t(0)
     tc = cfg.to_c()
     ctx.check(ctx.lib.rgs_densify_and_prune(ctx.handle, _fp(g), n, _fp(state.grad_accum), state.grad_denom.ctypes.data_as(L.U32P),
@@ -612,6 +622,13 @@ class Trainer:
         pick = {"tile": f"{chosen.tile_w}x{chosen.tile_h}", "batch": chosen.batch,
                 "pixels_per_thread": chosen.pixels_per_thread}
         return pick, table
+
+    def evaluated_pairs(self) -> tuple[int, int]:
+        """(forward, backward) (pixel, splat) pairs the blend kernels evaluated
+        in the last batched pass (the FP32 roofline's work count)."""
+        f, b = C.c_uint64(0), C.c_uint64(0)
+        self.ctx.check(self.lib.rgs_trainer_evaluated_pairs(self.ctx.handle, C.byref(f), C.byref(b)))
+        return int(f.value), int(b.value)
 
     def grads(self) -> np.ndarray:
         out = np.zeros((max(len(self), 1), GRAD_FLOATS), np.float32)

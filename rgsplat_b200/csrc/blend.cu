@@ -543,6 +543,43 @@ static void launch(const BlendArgs& a, int tw, int th, int batch, bool fwd, cuda
     k<<<grid, threads, 0, st>>>(a);
 }
 
+// (pixel, splat) pairs the blend evaluates, per pixel of view blockIdx.y: the
+// forward walks the pixel's tile list until T < 1e-4 ends it at its last
+// contributor (final T below 1e-4) or the list runs out; the backward walks
+// from the last contributor down to the front. out[0] += forward pairs,
+// out[1] += backward pairs.
+__global__ void __launch_bounds__(256) k_evaluated_pairs(const DevCam* __restrict__ cams, const uint2* __restrict__ ranges,
+                                                         const float* __restrict__ final_t, const int* __restrict__ last,
+                                                         int tile_w, int tile_h, unsigned long long* out) {
+    const DevCam& c = cams[blockIdx.y];
+    const uint32_t px = (uint32_t)c.width * (uint32_t)c.height;
+    unsigned long long f = 0, b = 0;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < px; p += gridDim.x * blockDim.x) {
+        const uint32_t x = p % (uint32_t)c.width, y = p / (uint32_t)c.width;
+        const uint2 r = ranges[c.tile_base + (y / tile_h) * c.tiles_x + x / tile_w];
+        const int l = last[(size_t)c.pix_base + p];
+        const float t = final_t[(size_t)c.pix_base + p];
+        f += t < 1e-4f ? (unsigned long long)(l + 1) : (unsigned long long)(r.y - r.x);
+        b += l >= 0 ? (unsigned long long)(l + 1) : 0ull;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        f += __shfl_down_sync(0xffffffffu, f, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    if ((threadIdx.x & 31) == 0 && (f | b)) {
+        atomicAdd(out, f);
+        atomicAdd(out + 1, b);
+    }
+}
+
+void launch_evaluated_pairs(const DevCam* cams, int nviews, const uint2* ranges, const float* final_t, const int* last,
+                            int tile_w, int tile_h, unsigned long long* out, cudaStream_t st) {
+    if (nviews <= 0) return;
+    k_evaluated_pairs<<<dim3((unsigned)device_sm_count() * 2, (unsigned)nviews), 256, 0, st>>>(cams, ranges, final_t, last,
+                                                                                            tile_w, tile_h, out);
+}
+
 void launch_blend_forward(const BlendArgs& a, int tw, int th, int batch, cudaStream_t st) { launch(a, tw, th, batch, true, st); }
 void launch_blend_backward(const BlendArgs& a, int tw, int th, int batch, cudaStream_t st) { launch(a, tw, th, batch, false, st); }
 

@@ -90,6 +90,8 @@ struct rgs_ctx {
     DBuf pkeys, pvals;
     uint32_t pair_cap = 0;
     bool split_hint = false;  // the last batched step ran as view groups
+    int batch_views = 0;      // views whose pixels the buffers hold from the last
+                              // batched pass run as one group (0: none)
     DBuf ranges, rgb, final_t, last, dl, partials;
     DBuf scalars, block_sums, view_pairs;
     SortScratch sort;
@@ -101,6 +103,7 @@ struct rgs_ctx {
     cudaGraphExec_t gexec = nullptr;
     std::vector<uint64_t> g_key;
     rgs_stats stats{};
+    MemCounter mem;  // device bytes held through this context's buffers
     cudaStream_t own_stream = nullptr;
     // host-target steps: targets copied on copy_st, the loss waits on ev_copy
     cudaStream_t copy_st = nullptr;
@@ -372,6 +375,8 @@ int ensure_work(rgs_ctx* ctx, size_t S, size_t px, size_t tiles, size_t lblocks,
     CK(ctx->hdr.ensure(sizeof(StepHdr)));
     CK(ctx->outd.ensure(sizeof(StepOut)));
     (void)V;
+    // whatever runs next writes the pixel buffers
+    ctx->batch_views = 0;
     return RGS_OK;
 }
 
@@ -608,6 +613,7 @@ int run_view_plain(rgs_ctx* ctx, Scene& s, const DevCam& dc_in, const float* tar
 
 int check_ctx(rgs_ctx* ctx) {
     if (!ctx) return RGS_ERR_INVALID_ARG;
+    t_mem = &ctx->mem;
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
     return RGS_OK;
@@ -678,6 +684,7 @@ int rgs_create(const rgs_options* opts, rgs_ctx** out) {
     rgs_ctx* ctx = new rgs_ctx();
     ctx->opt = o;
     ctx->device = o.device;
+    t_mem = &ctx->mem;
     cudaError_t e = cudaSetDevice(o.device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, o.device);
     // one-time per-device kernel attributes, set here so that no later call
@@ -707,6 +714,7 @@ int rgs_create(const rgs_options* opts, rgs_ctx** out) {
 void rgs_destroy(rgs_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
+    t_mem = &ctx->mem;
     if (ctx->st) cudaStreamSynchronize(ctx->st);
     if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
     Scene* ss[2] = {&ctx->tr, &ctx->sc};
@@ -730,6 +738,7 @@ void rgs_destroy(rgs_ctx* ctx) {
     if (ctx->ev_copy) cudaEventDestroy(ctx->ev_copy);
     if (ctx->copy_st) cudaStreamDestroy(ctx->copy_st);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    t_mem = nullptr;
     delete ctx;
 }
 
@@ -765,6 +774,15 @@ int rgs_get_stage_times(rgs_ctx* ctx, float* ms_out, int reset) {
         for (int i = 0; i < RGS_NUM_STAGES; ++i) ms_out[i] = ctx->stage_ms[i];
     if (reset)
         for (int i = 0; i < RGS_NUM_STAGES; ++i) ctx->stage_ms[i] = 0.0f;
+    return RGS_OK;
+}
+
+int rgs_get_memory(rgs_ctx* ctx, uint64_t* held_bytes, uint64_t* peak_bytes, int reset_peak) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (held_bytes) *held_bytes = ctx->mem.held;
+    if (peak_bytes) *peak_bytes = ctx->mem.peak;
+    if (reset_peak) ctx->mem.peak = ctx->mem.held;
     return RGS_OK;
 }
 
@@ -1527,6 +1545,7 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
             if (losses)
                 for (int v = 0; v < V; ++v) losses[v] = ctx->out_h->losses[v];
             if (fused) s.mlen = std::max(s.mlen, s.n);
+            ctx->batch_views = allow_split ? V : 0;
             return RGS_OK;
         }
         // pair buffer too small: Adam was skipped on the device; grow and
@@ -1574,6 +1593,7 @@ int split_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], fl
     }
     ctx->stats.pairs = total;
     ctx->stats.view_groups = (uint32_t)groups;
+    ctx->batch_views = 0;
     if (!fused) return RGS_OK;
     int rc = apply_adam(ctx, tc, (uint32_t)V);
     if (rc) return rc;
@@ -2137,6 +2157,39 @@ int rgs_debug_backward(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs
         CK(cudaMemcpyAsync(dl_dpix, ctx->dl.p, px * 12, cudaMemcpyDeviceToHost, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
     }
+    return RGS_OK;
+}
+
+int rgs_trainer_evaluated_pairs(rgs_ctx* ctx, uint64_t* forward_pairs, uint64_t* backward_pairs) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!forward_pairs || !backward_pairs) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
+    if (ctx->batch_views <= 0) return fail(ctx, RGS_ERR_INVALID_ARG, "no batched pass holds the pixel buffers");
+    const DevCam* cams_dev = (const DevCam*)((char*)ctx->hdr.p + offsetof(StepHdr, cams));
+    unsigned long long* out = ctx->view_pairs.as<unsigned long long>();
+    unsigned long long h[2] = {0, 0};
+    CK(cudaMemsetAsync(out, 0, 16, ctx->st));
+    launch_evaluated_pairs(cams_dev, ctx->batch_views, ctx->ranges.as<uint2>(), ctx->final_t.as<float>(), ctx->last.as<int>(),
+                           ctx->opt.tile_w, ctx->opt.tile_h, out, ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h, out, 16, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    *forward_pairs = h[0];
+    *backward_pairs = h[1];
+    return RGS_OK;
+}
+
+int rgs_debug_trainer_batch_pixels(rgs_ctx* ctx, size_t k, float* rgb, float* final_t, float* dl_dpix) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (ctx->batch_views <= 0) return fail(ctx, RGS_ERR_INVALID_ARG, "no batched pass holds the pixel buffers");
+    if (k >= (size_t)ctx->batch_views) return fail(ctx, RGS_ERR_INVALID_ARG, "view position out of range");
+    const DevCam& c = ctx->hdr_h->cams[k];
+    const size_t px = (size_t)c.width * c.height, base = (size_t)c.pix_base;
+    if (rgb) CK(cudaMemcpyAsync(rgb, ctx->rgb.as<float>() + base * 3, px * 12, cudaMemcpyDeviceToHost, ctx->st));
+    if (final_t) CK(cudaMemcpyAsync(final_t, ctx->final_t.as<float>() + base, px * 4, cudaMemcpyDeviceToHost, ctx->st));
+    if (dl_dpix) CK(cudaMemcpyAsync(dl_dpix, ctx->dl.as<float>() + base * 3, px * 12, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
     return RGS_OK;
 }
 

@@ -1,12 +1,15 @@
 // device.cu -- per-device facts the launchers size their grids from, looked up
 // once per device ordinal under a mutex, so a process that drives several GPUs
 // (one context per device, or the no-allocation loss on more than one device)
-// never reuses one device's answer for another.
+// never reuses one device's answer for another; and the calling thread's
+// device-memory counter (the context whose entry point is running).
 #include <mutex>
 
 #include "rgs_internal.cuh"
 
 namespace rgs {
+
+thread_local MemCounter* t_mem = nullptr;
 
 namespace {
 constexpr int MAX_DEVICES = 64;

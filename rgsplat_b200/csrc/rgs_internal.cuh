@@ -78,22 +78,44 @@ enum Status {
     E_NODEVICE = -7,
 };
 
+// Device bytes a context holds through its buffers, and the most it has held
+// since its last reset. Each entry point sets the calling thread's counter to
+// its context's (contexts are used by one host thread at a time).
+struct MemCounter {
+    size_t held = 0, peak = 0;
+};
+extern thread_local MemCounter* t_mem;
+inline void mem_add(size_t b) {
+    if (!t_mem) return;
+    t_mem->held += b;
+    if (t_mem->held > t_mem->peak) t_mem->peak = t_mem->held;
+}
+inline void mem_sub(size_t b) {
+    if (t_mem) t_mem->held -= b < t_mem->held ? b : t_mem->held;
+}
+
 // Grow-only device allocation.
 struct DBuf {
     void* p = nullptr;
     size_t bytes = 0;
     cudaError_t ensure(size_t need) {
         if (need <= bytes) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
+        release();
         size_t want = need + need / 4 + 256;
         cudaError_t e = cudaMalloc(&p, want);
-        if (e == cudaSuccess) bytes = want;
+        if (e == cudaSuccess) {
+            bytes = want;
+            mem_add(want);
+        } else {
+            p = nullptr;
+        }
         return e;
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            cudaFree(p);
+            mem_sub(bytes);
+        }
         p = nullptr;
         bytes = 0;
     }
@@ -201,6 +223,11 @@ struct BlendArgs {
 void launch_blend_forward(const BlendArgs& a, int tile_w, int tile_h, int batch, cudaStream_t st);
 void launch_blend_backward(const BlendArgs& a, int tile_w, int tile_h, int batch, cudaStream_t st);
 void launch_blend_store_all(const BlendArgs& a, bool fwd, cudaStream_t st);
+// (pixel, splat) pairs the forward and backward blends of a pass evaluated,
+// from its final T, last contributors and tile ranges: out[0] forward,
+// out[1] backward (added to; u64).
+void launch_evaluated_pairs(const DevCam* cams, int nviews, const uint2* ranges, const float* final_t, const int* last,
+                            int tile_w, int tile_h, unsigned long long* out, cudaStream_t st);
 
 // raster.cu: preview framebuffer (colour, 1 - T) as RGBA f32 or sRGB RGBA8.
 void launch_pack_framebuffer(const float* rgb, const float* final_t, size_t npix, int srgb8, void* out, cudaStream_t st);

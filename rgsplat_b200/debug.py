@@ -71,3 +71,16 @@ def backward(gaussians, camera: Camera, target_rgba, bg=(0.0, 0.0, 0.0), lam: fl
     tgt = _f32(target_rgba).reshape(-1)
     ctx.check(ctx.lib.rgs_debug_backward(ctx.handle, _fp(g), n, C.byref(cam), _fp(tgt), _fp(_f32(bg)), float(lam), _fp(acc), _fp(dl)))
     return acc[:n], dl
+
+
+def trainer_batch_pixels(trainer, views, k: int):
+    """View at position k of the trainer's last batched pass over ``views``, read
+    from the batch's own buffers -> (rgb (H, W, 3), final_t (H, W),
+    dL/dpixel (H, W, 3))."""
+    ctx = trainer.ctx
+    c = trainer.cameras[views[k]]
+    rgb = np.zeros((c.height, c.width, 3), np.float32)
+    ft = np.zeros((c.height, c.width), np.float32)
+    dl = np.zeros((c.height, c.width, 3), np.float32)
+    ctx.check(ctx.lib.rgs_debug_trainer_batch_pixels(ctx.handle, int(k), _fp(rgb), _fp(ft), _fp(dl)))
+    return rgb, ft, dl

@@ -70,12 +70,28 @@ class ViewParallelStep:
             return self.trainer.grad_tensor()
         return trainer_grad_tensor(self.trainer, self.device)
 
+    def _order_after_collective(self) -> None:
+        """The all-reduce is enqueued on torch's current stream; the update runs
+        on the library context's stream. Unless they are the same stream, the
+        host waits for the collective before the update is issued, so Adam
+        never reads gradient planes the collective is still writing."""
+        ctx = getattr(self.trainer, "ctx", None)
+        if ctx is None or self.device is None:
+            return
+        import torch
+
+        cur = torch.cuda.current_stream(self.device)
+        if getattr(ctx, "stream", None) != cur.cuda_stream:
+            cur.synchronize()
+
     def __call__(self, views: Sequence[int], loss_cfg=None, train_cfg=None):
         kw = {"loss_cfg": loss_cfg}
         if self.mode is not None:
             kw["mode"] = self.mode
+        # the backward returns with its work finished (it reads the losses back)
         losses = self.trainer.backward(list(views), **kw)
         if self.world > 1:
             self.dist.all_reduce(self._grad(), group=self.group)
+            self._order_after_collective()
         self.trainer.apply_adam(train_cfg, denom_increment=len(views) * self.world)
         return losses

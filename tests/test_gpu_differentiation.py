@@ -114,3 +114,22 @@ def test_store_all_backward_matches_recompute(workload, ctx):
     assert r0["state_bytes"] == px * 8
     assert r1["state_bytes"] == px * 8 + r1["pairs"] * 256 * 4
     assert r0["backward_ms"] > 0 and r1["backward_ms"] > 0
+
+
+def test_store_all_needs_more_device_memory(workload):
+    """The peak device memory of each backward variant: a fresh context's
+    high-water mark over one call holds at least the variant's blend state,
+    and the store-all variant's exceeds the recompute variant's by about its
+    per-(pair, pixel) T store."""
+    g, cam, target, _ = workload
+    peaks, state = {}, {}
+    for store in (False, True):
+        c = R.Context()
+        assert c.memory()["peak_bytes"] == c.memory()["held_bytes"]
+        _, _, r = R.render_and_backward_variant(g, cam, target, store_all=store, ctx=c)
+        m = c.memory(reset_peak=True)
+        assert m["peak_bytes"] >= m["held_bytes"] >= r["state_bytes"]
+        assert c.memory()["peak_bytes"] == m["held_bytes"]
+        peaks[store], state[store] = m["peak_bytes"], r["state_bytes"]
+        c.close()
+    assert peaks[True] - peaks[False] >= 0.9 * (state[True] - state[False])

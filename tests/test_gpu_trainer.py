@@ -386,3 +386,41 @@ def test_stage_profiling_and_external_stream():
     assert ms["forward"] > 0 and ms["backward"] > 0 and ms["geometry_adam"] > 0
     tr.ctx.set_stream(None)
     tr.step([1, 2], mode=R.Trainer.BATCHED)
+
+
+def oracle_evaluated_pairs(g, cam, bg):
+    """(pixel, splat) pairs forward_pass and backward_pass evaluate
+    (backward.rs:296-512): the forward walks a pixel's tile list until T < 1e-4
+    at its last contributor or to the end, the backward from the last
+    contributor to the front."""
+    _, ft, last = O.render_color(g, cam, bg)
+    offs, _ = O.tile_lists(g, cam)
+    tx = (cam.width + 15) // 16
+    ys, xs = np.mgrid[0:cam.height, 0:cam.width]
+    t = (ys // 16) * tx + xs // 16
+    length = (offs[1:] - offs[:-1])[t]
+    fwd = np.where(ft < 1e-4, last + 1, length).astype(np.int64).sum()
+    bwd = np.where(last >= 0, last + 1, 0).astype(np.int64).sum()
+    return int(fwd), int(bwd)
+
+
+def test_evaluated_pairs_counter_matches_oracle():
+    """rgs_trainer_evaluated_pairs after a batched pass: with a non-zero
+    background the blend walks the reference's full tile lists, so the counts
+    equal the oracle's; with a zero background the lists are pruned to each
+    row's reachable span and the counts can only be smaller."""
+    g, cams, targets = multi_view_scene(seed=25)
+    views = [0, 2, 5]
+    tr = R.Trainer(g, cams, targets)
+    bg = (0.1, 0.2, 0.3)
+    tr.backward(views, bg=bg, mode=R.Trainer.BATCHED)
+    f, b = tr.evaluated_pairs()
+    want = [oracle_evaluated_pairs(g, cams[v], bg) for v in views]
+    assert (f, b) == (sum(w[0] for w in want), sum(w[1] for w in want))
+    assert f >= b > 0
+    tr.backward(views, mode=R.Trainer.BATCHED)
+    fp, bp = tr.evaluated_pairs()
+    assert 0 < fp <= f and 0 < bp <= b
+    tr.step(views, mode=R.Trainer.PLAIN)
+    with pytest.raises(R.RgsError):
+        tr.evaluated_pairs()  # a plain step rewrote the pixel buffers

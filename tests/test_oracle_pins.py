@@ -264,7 +264,7 @@ def test_exp_edge_cases():
 
 
 def test_linear_srgb():
-    """src/cpu/rasterizer.rs:275-281 (test_linear_srgb)."""
+    """src/cpu/rasterizer.rs:285-290 (test_linear_srgb)."""
     v = O.linear_to_srgb([0.0, 1.0, 0.5])
     assert abs(v[0] - 0.0) < 1e-6
     assert abs(v[1] - 1.0) < 1e-6
@@ -346,7 +346,7 @@ def _ply_roundtrip_scene():
 
 
 def test_ply_roundtrip_preserves_parameters():
-    """src/io/ply.rs:290-320 (ply_roundtrip_preserves_parameters)."""
+    """src/io/ply.rs:309-335 (ply_roundtrip_preserves_parameters)."""
     orig = _ply_roundtrip_scene()
     back = O.load_ply_bytes(O.save_ply_bytes(orig))
     assert back.shape == orig.shape
@@ -359,7 +359,7 @@ def test_ply_roundtrip_preserves_parameters():
 
 
 def test_splat_record_is_32_bytes():
-    """src/io/ply.rs:322-330 (splat_record_is_32_bytes)."""
+    """src/io/ply.rs:337-345 (splat_record_is_32_bytes)."""
     from tests import refcases as RC
 
     g = np.stack([RC.gaussian_new([0.0, 0.0, 0.0])] * 10)
