@@ -39,6 +39,13 @@ int rgs_debug_forward(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_
 int rgs_debug_backward(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, const float* target_rgba,
                        const float bg[3], float lambda, float* acc9, float* dl_dpix);
 
+/* Largest relative difference between the backward blend's SFU exponential
+ * and the forward's exact exp (the one the oracle restates) over n points on
+ * [lo, hi], -8 <= lo <= hi <= 0: the bound behind the backward's rule of
+ * deciding alpha >= 1/255 and alpha > 0.99 with the exact exp whenever the
+ * SFU value lies within 4e-6 relative of either threshold. */
+int rgs_debug_exp_sfu_error(rgs_ctx* ctx, float lo, float hi, uint32_t n, float* max_rel);
+
 /* Pixels of the view at position k of the trainer's most recent batched pass
  * (rgs_trainer_step or rgs_trainer_backward with RGS_STEP_BATCHED that ran as
  * one view group), read from the batch's own buffers: rgb w*h*3, final T w*h

@@ -220,6 +220,7 @@ SIGNATURES = {
     "rgs_debug_forward": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), FP, FP, FP, C.POINTER(C.c_int32)]),
     "rgs_debug_backward": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), FP, FP, C.c_float, FP, FP]),
     "rgs_debug_trainer_batch_pixels": (C.c_int, [CTX, C.c_size_t, FP, FP, FP]),
+    "rgs_debug_exp_sfu_error": (C.c_int, [CTX, C.c_float, C.c_float, C.c_uint32, FP]),
 }
 
 

@@ -305,8 +305,10 @@ __device__ __forceinline__ void red_add_v4(float4* addr, float x, float y, float
 // serves both uses, where the reference divides, backward.rs:452): over the
 // at most few hundred splats a pixel rebuilds through, T stays within ~1e-5
 // relative of the reference's, far inside the gradients' 1e-3 tolerance.
-// Alpha itself is recomputed bit for bit as the forward did, so the set of
-// contributing splats is the forward's.
+// Alpha is formed with the SFU exponential (within 1e-6 of the forward's
+// value); wherever that value lies within 4e-6 relative of the 1/255 cut or
+// the 0.99 clamp, the forward's exact exp decides instead, so the set of
+// contributing splats and the clamped ones are exactly the forward's.
 // The register budget is capped for occupancy: eight 128-thread CTAs per SM
 // with two pixels per thread, twelve 64-thread CTAs with four (a few spilled
 // words cost less than the lost warps: measured 2 % and 10 % faster backward
@@ -407,8 +409,17 @@ __global__ void __launch_bounds__(TW * TH / PPT, PPT == 2 ? 8 : PPT == 4 ? 12 : 
                         const float dy = pyc[p] - A.y;
                         const float power = -0.5f * (tdx + t2b * dy + Q.z * dy * dy);
                         if (power > 0.0f || power < A.w) continue;
-                        const float g_exp = expf_fast_nonpos(power);
-                        const float alpha_raw = A.z * g_exp;
+                        // alpha to ~1e-6 from the SFU exponential; where that cannot
+                        // settle the forward's decisions (alpha >= 1/255, alpha_raw >
+                        // 0.99), the forward's own exp settles them, so the
+                        // contributing set is exactly the forward's
+                        float g_exp = exp_sfu_nonpos(power);
+                        float alpha_raw = A.z * g_exp;
+                        if (fabsf(alpha_raw - 1.0f / 255.0f) < SFU_BAND * (1.0f / 255.0f) ||
+                            fabsf(alpha_raw - 0.99f) < SFU_BAND * 0.99f) {
+                            g_exp = expf_fast_nonpos(power);
+                            alpha_raw = A.z * g_exp;
+                        }
                         const float alpha = fminf(alpha_raw, 0.99f);
                         if (alpha < 1.0f / 255.0f) continue;
                         float inv_1ma;
@@ -571,6 +582,25 @@ __global__ void __launch_bounds__(256) k_evaluated_pairs(const DevCam* __restric
         atomicAdd(out, f);
         atomicAdd(out + 1, b);
     }
+}
+
+// Largest |exp_sfu_nonpos(x) / expf_fast_nonpos(x) - 1| over n points spaced
+// evenly on [lo, hi] (hi <= 0), as float bits in *out (non-negative floats
+// order like their bits).
+__global__ void k_exp_sfu_error(float lo, float hi, uint32_t n, unsigned int* out) {
+    float m = 0.0f;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float x = lo + (hi - lo) * ((float)i / (float)(n > 1 ? n - 1 : 1));
+        const float e = expf_fast_nonpos(x);
+        m = fmaxf(m, fabsf(exp_sfu_nonpos(x) / e - 1.0f));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+void launch_exp_sfu_error(float lo, float hi, uint32_t n, unsigned int* out, cudaStream_t st) {
+    k_exp_sfu_error<<<device_sm_count() * 4, 256, 0, st>>>(lo, hi, n, out);
 }
 
 void launch_evaluated_pairs(const DevCam* cams, int nviews, const uint2* ranges, const float* final_t, const int* last,

@@ -2179,6 +2179,23 @@ int rgs_trainer_evaluated_pairs(rgs_ctx* ctx, uint64_t* forward_pairs, uint64_t*
     return RGS_OK;
 }
 
+int rgs_debug_exp_sfu_error(rgs_ctx* ctx, float lo, float hi, uint32_t n, float* max_rel) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!max_rel || n == 0 || !(lo <= hi) || !(hi <= 0.0f) || !(lo >= -8.0f))
+        return fail(ctx, RGS_ERR_INVALID_ARG, "need -8 <= lo <= hi <= 0, n > 0");
+    CK(ctx->view_pairs.ensure(MAX_VIEWS * 8));
+    unsigned int* out = ctx->view_pairs.as<unsigned int>();
+    unsigned int h = 0;
+    CK(cudaMemsetAsync(out, 0, 4, ctx->st));
+    launch_exp_sfu_error(lo, hi, n, out, ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(&h, out, 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    std::memcpy(max_rel, &h, 4);
+    return RGS_OK;
+}
+
 int rgs_debug_trainer_batch_pixels(rgs_ctx* ctx, size_t k, float* rgb, float* final_t, float* dl_dpix) {
     int rc = check_ctx(ctx);
     if (rc) return rc;

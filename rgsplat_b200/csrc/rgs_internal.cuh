@@ -223,6 +223,9 @@ struct BlendArgs {
 void launch_blend_forward(const BlendArgs& a, int tile_w, int tile_h, int batch, cudaStream_t st);
 void launch_blend_backward(const BlendArgs& a, int tile_w, int tile_h, int batch, cudaStream_t st);
 void launch_blend_store_all(const BlendArgs& a, bool fwd, cudaStream_t st);
+// Largest relative difference of the backward's SFU exponential from the
+// forward's exp over n points on [lo, hi] (float bits, atomicMax into *out).
+void launch_exp_sfu_error(float lo, float hi, uint32_t n, unsigned int* out, cudaStream_t st);
 // (pixel, splat) pairs the forward and backward blends of a pass evaluated,
 // from its final T, last contributors and tile ranges: out[0] forward,
 // out[1] backward (added to; u64).

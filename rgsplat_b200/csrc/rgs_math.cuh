@@ -177,6 +177,23 @@ __device__ __forceinline__ float expf_fast_nonpos(float x) {
     return p * __int_as_float(((int)k + 127) << 23);
 }
 
+// e^x for x in [-8, 0] from the special-function unit's base-2 exponential
+// (PTX ex2.approx.ftz.f32) of x * log2(e): one multiply and one SFU
+// instruction, within a few ulp (relative error below 1e-6 on that range,
+// checked against expf_fast_nonpos by a GPU test). For values that only need
+// to be close, never for a decision that must match the forward pass.
+__device__ __forceinline__ float exp_sfu_nonpos(float x) {
+    const float y = x * 1.44269504f;
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(y));
+    return r;
+}
+
+// Relative half-width of the band around a threshold inside which an alpha
+// formed with exp_sfu_nonpos cannot decide which side the forward's exact
+// alpha lies on (4x the tested error bound of exp_sfu_nonpos).
+constexpr float SFU_BAND = 4e-6f;
+
 // Rust f32::max / f32::min ignore a NaN operand (fmaxf/fminf do the same);
 // f32::clamp propagates NaN.
 __device__ __forceinline__ float rclamp(float x, float lo, float hi) {

@@ -84,3 +84,12 @@ def trainer_batch_pixels(trainer, views, k: int):
     dl = np.zeros((c.height, c.width, 3), np.float32)
     ctx.check(ctx.lib.rgs_debug_trainer_batch_pixels(ctx.handle, int(k), _fp(rgb), _fp(ft), _fp(dl)))
     return rgb, ft, dl
+
+
+def exp_sfu_error(lo: float = -8.0, hi: float = 0.0, n: int = 1 << 24, ctx: Context | None = None) -> float:
+    """Largest relative difference of the backward's SFU exponential from the
+    forward's exp over n points on [lo, hi]."""
+    ctx = ctx or default_context()
+    out = np.zeros(1, np.float32)
+    ctx.check(ctx.lib.rgs_debug_exp_sfu_error(ctx.handle, float(lo), float(hi), int(n), _fp(out)))
+    return float(out[0])

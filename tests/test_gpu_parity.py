@@ -330,3 +330,14 @@ def test_trainer_rasterize_matches_oracle(bg):
     fb2 = tr.rasterize(0, bg)
     assert np.array_equal(fb2.reshape(-1).view(np.uint32), O.rasterize(g2, cam, bg).reshape(-1).view(np.uint32))
     assert np.array_equal(tr.rasterize(0, bg, srgb8=True), O.to_u8_srgb(fb2))
+
+
+def test_backward_sfu_exponential_error_bound():
+    """The backward blend forms alpha with the SFU's base-2 exponential and
+    defers to the forward's exact exp whenever that value lies within 4e-6
+    relative of the 1/255 cut or the 0.99 clamp, so that it contributes
+    exactly the splats the forward did. That needs the SFU value within 1e-6
+    of the exact one on the whole range the blend uses (power in [-8, 0])."""
+    e = D.exp_sfu_error(-8.0, 0.0, 1 << 24)
+    assert 0.0 <= e < 1e-6, e
+    assert D.exp_sfu_error(-6.0, -5.0, 1 << 22) < 1e-6

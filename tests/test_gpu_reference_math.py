@@ -16,7 +16,10 @@ arithmetic, and the CUDA results are held to the north_star bars against it:
   whose last contributor agrees; pixels where an alpha >= 1/255 or T < 1e-4
   decision flipped (counted by the last contributor) at most 1 per 100k
   pixels plus 2;
-* loss within 1e-4 relative, every gradient group within 1e-3 relative.
+* loss within 1e-4 relative of the reference image's loss summed in double
+  (the reference's own serial f32 sum drifts by percents on a 1600x1064
+  image, so its value is no bar there), every gradient group within 1e-3
+  relative.
 
 Workloads: the 10k-Gaussian 256x256 view, the 50k-Gaussian 512x512 view and
 one 1600x1064 view of the 1M-Gaussian scene. The flip counts are printed
@@ -95,13 +98,14 @@ def test_cuda_path_against_libm_reference_math(case, libm):
     t_err = float(np.abs(ft - ref.final_t)[keep].max()) if keep.any() else 0.0
     rel = {k: float(np.linalg.norm(grads[:, s] - ref.grads[:, s]) / max(np.linalg.norm(ref.grads[:, s]), 1e-30))
            for k, s in GROUPS.items()}
+    exact, _ = O.photometric_loss_grad(ref.rendered, target, cam.width, cam.height, 0.2, double=True)
     print(f"\n[{case}] pairs {pairs}, tile-list flips {tflips}; pixels {px}, last-contributor flips {npf}; "
-          f"image max abs {img_err:.3e}, final T max abs {t_err:.3e}; loss rel "
-          f"{abs(loss - ref.loss) / ref.loss:.3e}; gradient rel " + ", ".join(f"{k} {v:.2e}" for k, v in rel.items()))
+          f"image max abs {img_err:.3e}, final T max abs {t_err:.3e}; loss rel to the double sum "
+          f"{abs(loss - exact) / exact:.3e} (reference's f32 sum {abs(ref.loss - exact) / exact:.3e}); gradient rel " + ", ".join(f"{k} {v:.2e}" for k, v in rel.items()))
 
     assert tflips <= pairs // 1_000_000 + 2
     assert npf <= px // 100_000 + 2
     assert img_err <= 1e-4 and t_err <= 1e-4
-    assert abs(loss - ref.loss) <= 1e-4 * ref.loss
+    assert abs(loss - exact) <= 1e-4 * exact
     for k, e in rel.items():
         assert e < 1e-3, f"{k}: {e:.2e}"
