@@ -132,6 +132,10 @@ template <int TW, int TH, int BATCH, bool RECT, int PPT, bool STORE = false>
 __global__ void __launch_bounds__(TW * TH / PPT) k_blend_fwd(BlendArgs a) {
     constexpr int NT = TW * TH / PPT;
     constexpr bool ROWTERMS = RowTerms<BATCH, TH, PPT>::on;
+    // two pixels per thread in packed f32x2 lanes (the store-all study keeps
+    // the scalar loop)
+    constexpr bool PACK = PPT == 2 && !STORE;
+    const float2 one2 = make_float2(a.one, a.one);
     __shared__ float4 s_a[BATCH];
     __shared__ float4 s_c[BATCH];
     __shared__ float4 s_k[BATCH];
@@ -210,6 +214,57 @@ __global__ void __launch_bounds__(TW * TH / PPT) k_blend_fwd(BlendArgs a) {
 #pragma unroll
                 for (int h = 0; h < (PPT + 1) / 2; ++h)
                     rw[h] = ROWTERMS ? *reinterpret_cast<const float4*>(&s_row[k][rbase + 2 * h]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                if (PACK && !a.bg_start) {
+                    // both pixels in packed f32x2 lanes, each lane rounded exactly as
+                    // the scalar loop below rounds that pixel; a pixel that does not
+                    // take this splat gets alpha = 0, which leaves its colour
+                    // (+0 added to a non-negative sum) and T (times 1) unchanged
+                    float2 dy2, qdd2;
+                    if (ROWTERMS) {
+                        dy2 = make_float2(rw[0].x, rw[0].z);
+                        qdd2 = make_float2(rw[0].y, rw[0].w);
+                    } else {
+                        dy2 = __fadd2_rn(make_float2(pyc[0], pyc[PPT > 1 ? 1 : 0]), bc2(-A.y));
+                        qdd2 = __fmul2_rn(__fmul2_rn(bc2(Q.z), dy2), dy2);
+                    }
+                    // power = -0.5 * ((tdx + t2b * dy) + qdd)
+                    const float2 s1 = __ffma2_rn(__fmul2_rn(bc2(t2b), dy2), one2, bc2(tdx));
+                    const float2 s2 = ROWTERMS ? __fadd2_rn(s1, qdd2) : __ffma2_rn(qdd2, one2, s1);
+                    const float2 pw = __fmul2_rn(s2, bc2(-0.5f));
+                    bool act0 = !done[0] && !(pw.x > 0.0f) && !(pw.x < A.w);
+                    bool act1 = !done[PPT > 1 ? 1 : 0] && !(pw.y > 0.0f) && !(pw.y < A.w);
+                    if (RECT) {
+                        act0 = act0 && in_rect(Q.w, s_k[k].w, px, py0);
+                        act1 = act1 && in_rect(Q.w, s_k[k].w, px, py0 + 1);
+                    }
+                    if (act0 || act1) {
+                        const float2 ar = __fmul2_rn(bc2(A.z), expf_fast_nonpos2(pw, one2));
+                        float al0 = fminf(ar.x, 0.99f), al1 = fminf(ar.y, 0.99f);
+                        act0 = act0 && !(al0 < 1.0f / 255.0f);
+                        act1 = act1 && !(al1 < 1.0f / 255.0f);
+                        if (act0 || act1) {
+                            const float4 K = s_k[k];
+                            const float2 al = make_float2(act0 ? al0 : 0.0f, act1 ? al1 : 0.0f);
+                            float2 T2 = make_float2(T[0], T[PPT > 1 ? 1 : 0]);
+                            const float2 w = __fmul2_rn(al, T2);
+                            const float2 c0 = __ffma2_rn(__fmul2_rn(bc2(K.x), w), one2, make_float2(C0[0], C0[PPT > 1 ? 1 : 0]));
+                            const float2 c1 = __ffma2_rn(__fmul2_rn(bc2(K.y), w), one2, make_float2(C1[0], C1[PPT > 1 ? 1 : 0]));
+                            const float2 c2 = __ffma2_rn(__fmul2_rn(bc2(K.z), w), one2, make_float2(C2[0], C2[PPT > 1 ? 1 : 0]));
+                            T2 = __fmul2_rn(T2, __ffma2_rn(al, make_float2(-one2.x, -one2.y), one2));
+                            C0[0] = c0.x; C1[0] = c1.x; C2[0] = c2.x; T[0] = T2.x;
+                            C0[PPT - 1] = c0.y; C1[PPT - 1] = c1.y; C2[PPT - 1] = c2.y; T[PPT - 1] = T2.y;
+                            const int li = s_li[k];
+                            if (act0) {
+                                last[0] = li;
+                                if (T2.x < 1e-4f) done[0] = true;
+                            }
+                            if (act1) {
+                                last[PPT - 1] = li;
+                                if (T2.y < 1e-4f) done[PPT - 1] = true;
+                            }
+                        }
+                    }
+                } else {
 #pragma unroll
                 for (int p = 0; p < PPT; ++p) {
                     if (done[p]) continue;
@@ -235,6 +290,7 @@ __global__ void __launch_bounds__(TW * TH / PPT) k_blend_fwd(BlendArgs a) {
                     T[p] *= 1.0f - alpha;
                     last[p] = s_li[k];
                     if (T[p] < 1e-4f) done[p] = true;
+                }
                 }
                 all_done = true;
 #pragma unroll
@@ -317,6 +373,10 @@ template <int TW, int TH, int BATCH, bool RECT, int PPT, bool STORE = false>
 __global__ void __launch_bounds__(TW * TH / PPT, PPT == 2 ? 8 : PPT == 4 ? 12 : 1) k_blend_bwd(BlendArgs a) {
     constexpr int NT = TW * TH / PPT;
     constexpr int NACC = 9;
+    // pairs of pixels in packed f32x2 lanes (the store-all study keeps the
+    // scalar loop)
+    constexpr bool PACKB = PPT % 2 == 0 && !STORE;
+    const float2 one2 = make_float2(a.one, a.one);
     __shared__ float4 s_a[BATCH];
     __shared__ float4 s_c[BATCH];
     __shared__ float4 s_k[BATCH];
@@ -401,6 +461,83 @@ __global__ void __launch_bounds__(TW * TH / PPT, PPT == 2 ? 8 : PPT == 4 ? 12 : 
                     // per-entry factors of the conic / mean gradients
                     const float hdxx = -0.5f * dx * dx, qxdx = Q.x * dx, qydx = Q.y * dx;
                     float su = 0.0f, sud = 0.0f, sudd = 0.0f;  // sums over pixels of u, u dy, u dy^2
+                    if (PACKB) {
+                        // pixel pairs (p, p + 1) in packed f32x2 lanes; the power, and
+                        // with it every decision, is rounded per lane exactly as the
+                        // forward rounds it. A lane that does not take this splat
+                        // keeps its T and behind-colour sum and adds zeros.
+                        float2 G0 = bc2(0.0f), G1 = bc2(0.0f), G2 = bc2(0.0f), G3 = bc2(0.0f);
+                        float2 SU = bc2(0.0f), SUD = bc2(0.0f), SUDD = bc2(0.0f);
+#pragma unroll
+                        for (int h = 0; h < PPT / 2; ++h) {
+                            const int p0 = 2 * h, p1 = 2 * h + 1;
+                            bool a0 = li <= lc[p0], a1 = li <= lc[p1];
+                            if (RECT) {
+                                a0 = a0 && in_rect(Q.w, K.w, px, py0 + p0);
+                                a1 = a1 && in_rect(Q.w, K.w, px, py0 + p1);
+                            }
+                            if (!(a0 || a1)) continue;
+                            const float2 dy2 = __fadd2_rn(make_float2(pyc[p0], pyc[p1]), bc2(-A.y));
+                            const float2 qdd2 = __fmul2_rn(__fmul2_rn(bc2(Q.z), dy2), dy2);
+                            const float2 s1 = __ffma2_rn(__fmul2_rn(bc2(t2b), dy2), one2, bc2(tdx));
+                            const float2 pw = __fmul2_rn(__ffma2_rn(qdd2, one2, s1), bc2(-0.5f));
+                            a0 = a0 && !(pw.x > 0.0f) && !(pw.x < A.w);
+                            a1 = a1 && !(pw.y > 0.0f) && !(pw.y < A.w);
+                            if (!(a0 || a1)) continue;
+                            float2 ge = make_float2(exp_sfu_nonpos(pw.x), exp_sfu_nonpos(pw.y));
+                            float2 ar = __fmul2_rn(bc2(A.z), ge);
+                            if (fabsf(ar.x - 1.0f / 255.0f) < SFU_BAND * (1.0f / 255.0f) || fabsf(ar.x - 0.99f) < SFU_BAND * 0.99f) {
+                                ge.x = expf_fast_nonpos(pw.x);
+                                ar.x = A.z * ge.x;
+                            }
+                            if (fabsf(ar.y - 1.0f / 255.0f) < SFU_BAND * (1.0f / 255.0f) || fabsf(ar.y - 0.99f) < SFU_BAND * 0.99f) {
+                                ge.y = expf_fast_nonpos(pw.y);
+                                ar.y = A.z * ge.y;
+                            }
+                            const float al0 = fminf(ar.x, 0.99f), al1 = fminf(ar.y, 0.99f);
+                            a0 = a0 && !(al0 < 1.0f / 255.0f);
+                            a1 = a1 && !(al1 < 1.0f / 255.0f);
+                            if (!(a0 || a1)) continue;
+                            const float2 al = make_float2(a0 ? al0 : 0.0f, a1 ? al1 : 0.0f);
+                            const float2 om = __ffma2_rn(al, bc2(-1.0f), bc2(1.0f));
+                            const float2 inv = make_float2(__fdividef(1.0f, om.x), __fdividef(1.0f, om.y));
+                            float2 Tp = __fmul2_rn(make_float2(T[p0], T[p1]), inv);
+                            Tp = make_float2(a0 ? Tp.x : T[p0], a1 ? Tp.y : T[p1]);
+                            T[p0] = Tp.x;
+                            T[p1] = Tp.y;
+                            const float2 w = __fmul2_rn(al, Tp);
+                            const float2 d0 = make_float2(dl0[p0], dl0[p1]);
+                            const float2 d1 = make_float2(dl1[p0], dl1[p1]);
+                            const float2 d2 = make_float2(dl2[p0], dl2[p1]);
+                            G0 = __ffma2_rn(d0, w, G0);
+                            G1 = __ffma2_rn(d1, w, G1);
+                            G2 = __ffma2_rn(d2, w, G2);
+                            const float2 dk = __ffma2_rn(d2, bc2(K.z), __ffma2_rn(d1, bc2(K.y), __fmul2_rn(d0, bc2(K.x))));
+                            const float2 sb = make_float2(sbe[p0], sbe[p1]);
+                            const float2 dda = __ffma2_rn(Tp, dk, __fmul2_rn(make_float2(-sb.x, -sb.y), inv));
+                            const float2 sbn = __ffma2_rn(w, dk, sb);
+                            sbe[p0] = sbn.x;
+                            sbe[p1] = sbn.y;
+                            // zero for a lane that does not take the splat or whose raw
+                            // alpha was clamped (backward.rs:459-461)
+                            const float2 draw = make_float2(a0 && !(ar.x > 0.99f) ? dda.x : 0.0f, a1 && !(ar.y > 0.99f) ? dda.y : 0.0f);
+                            G3 = __ffma2_rn(draw, make_float2(a0 ? ge.x : 0.0f, a1 ? ge.y : 0.0f), G3);
+                            const float2 u = __fmul2_rn(draw, make_float2(a0 ? ar.x : 0.0f, a1 ? ar.y : 0.0f));
+                            SU = __fadd2_rn(SU, u);
+                            SUD = __ffma2_rn(u, dy2, SUD);
+                            SUDD = __ffma2_rn(__fmul2_rn(u, dy2), dy2, SUDD);
+                            contrib = true;
+                        }
+                        if (contrib) {
+                            g[0] = G0.x + G0.y;
+                            g[1] = G1.x + G1.y;
+                            g[2] = G2.x + G2.y;
+                            g[3] = G3.x + G3.y;
+                            su = SU.x + SU.y;
+                            sud = SUD.x + SUD.y;
+                            sudd = SUDD.x + SUDD.y;
+                        }
+                    } else {
 #pragma unroll
                     for (int p = 0; p < PPT; ++p) {
                         if (li > lc[p]) continue;
@@ -451,6 +588,7 @@ __global__ void __launch_bounds__(TW * TH / PPT, PPT == 2 ? 8 : PPT == 4 ? 12 : 
                         sud = __fmaf_rn(u, dy, sud);
                         sudd = __fmaf_rn(u * dy, dy, sudd);
                         contrib = true;
+                    }
                     }
                     if (contrib) {
                         g[4] = hdxx * su;

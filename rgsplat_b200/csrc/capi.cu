@@ -506,6 +506,7 @@ BlendArgs blend_args(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, cons
     a.pixels_per_thread = ctx->opt.pixels_per_thread;
     a.tstore = nullptr;
     a.bg_start = 0;
+    a.one = 1.0f;
     return a;
 }
 

@@ -219,6 +219,9 @@ struct BlendArgs {
     float* tstore;                 // store-all variant only: T per (list position, tile pixel)
     int bg_start;                  // preview compositing (rasterizer.rs:133): colour starts at bg and
                                    // the output is that sum, bg not scaled by the final T
+    float one;                     // 1.0f, read at run time: the packed-lane kernels add
+                                   // products as fma(product, one, acc) so that the code
+                                   // generator cannot fuse the multiply into the add
 };
 void launch_blend_forward(const BlendArgs& a, int tile_w, int tile_h, int batch, cudaStream_t st);
 void launch_blend_backward(const BlendArgs& a, int tile_w, int tile_h, int batch, cudaStream_t st);

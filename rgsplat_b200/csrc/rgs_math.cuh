@@ -177,6 +177,50 @@ __device__ __forceinline__ float expf_fast_nonpos(float x) {
     return p * __int_as_float(((int)k + 127) << 23);
 }
 
+// ---- two pixels at once: Blackwell's packed f32x2 instructions ------------
+// __fadd2_rn / __fmul2_rn / __ffma2_rn round each lane exactly like the scalar
+// _rn operation (one issue slot for two lanes), so a sequence of them gives
+// each lane the bits the same scalar sequence gives. One caveat, measured: the
+// code generator may contract a packed multiply feeding a packed add into a
+// packed FMA (one rounding instead of two), even without --fmad. Every such
+// add is therefore written as __ffma2_rn(product, one, acc), with `one` =
+// {1, 1} taken from a kernel argument, which it cannot fold: x * 1 + acc
+// rounds once, exactly like the separate add.
+__device__ __forceinline__ float2 bc2(float x) { return make_float2(x, x); }
+
+// expf_fast_nonpos on two lanes: the same operations in the same order per
+// lane (a negated operand moves to the exactly representable constant), so
+// each lane is bit-identical to the scalar routine. 2^k is assembled from the
+// shifted sum j, whose low mantissa bits hold k (bits(j) = bits(SHIFT) + k),
+// which is the same power of two the scalar routine builds from (int)k.
+__device__ __forceinline__ float2 expf_fast_nonpos2(float2 x, float2 one) {
+    const float L2E = 1.44269502f;
+    const float SHIFT = 12582912.0f;
+    const float LN2_HI = 0.693145751953125f;
+    const float LN2_LO = 1.42860677e-06f;
+    const float2 j = __ffma2_rn(x, bc2(L2E), bc2(SHIFT));
+    const float2 k = __fadd2_rn(j, bc2(-SHIFT));
+    const float2 rh = __ffma2_rn(k, bc2(-LN2_HI), x);
+    const float2 rl = __fmul2_rn(k, bc2(-LN2_LO));
+    float2 q = __ffma2_rn(bc2(2.48015873e-05f), rh, bc2(1.98412698e-4f));
+    q = __ffma2_rn(q, rh, bc2(1.38888889e-3f));
+    q = __ffma2_rn(q, rh, bc2(8.33333333e-3f));
+    q = __ffma2_rn(q, rh, bc2(4.16666667e-2f));
+    q = __ffma2_rn(q, rh, bc2(1.66666667e-1f));
+    q = __ffma2_rn(q, rh, bc2(0.5f));
+    const float2 hi = __fadd2_rn(one, rh);
+    const float2 omh = __ffma2_rn(hi, make_float2(-one.x, -one.y), one);  // 1 - hi, rounded once
+    const float2 lo = __fadd2_rn(omh, rh);
+    const float2 s = __fmul2_rn(rh, rh);
+    float2 tail = __ffma2_rn(s, q, lo);
+    const float2 ea = __fadd2_rn(hi, tail);
+    tail = __ffma2_rn(rl, ea, tail);
+    const float2 p = __fadd2_rn(hi, tail);
+    const float2 scale = make_float2(__int_as_float((__float_as_int(j.x) - 0x4B3FFF81) << 23),
+                                     __int_as_float((__float_as_int(j.y) - 0x4B3FFF81) << 23));
+    return __fmul2_rn(p, scale);
+}
+
 // e^x for x in [-8, 0] from the special-function unit's base-2 exponential
 // (PTX ex2.approx.ftz.f32) of x * log2(e): one multiply and one SFU
 // instruction, within a few ulp (relative error below 1e-6 on that range,
