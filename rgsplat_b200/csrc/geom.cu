@@ -382,6 +382,49 @@ __global__ void __launch_bounds__(128, PART == 2 ? 8 : 6) k_geom_gauss(const flo
     }
 }
 
+// The SH half of the fused geometry + Adam pass, one colour channel per grid
+// row (blockIdx.y): sum over views of mask_v[ch] * basis_v (the views in the
+// same order as k_geom_gauss<1, 1>, which adds the same products; a view whose
+// mask is zero for this channel adds only zeros there), then Adam on the
+// channel's four SH planes. Sixteen sums per thread instead of forty-eight,
+// so more warps stay resident in this latency-bound pass. Runs before the
+// geometry half, which rewrites the position it reads.
+__global__ void __launch_bounds__(128, 8) k_geom_sh(int n, int cap, const DevCam* __restrict__ cams, int nviews,
+                                                   const uint32_t* __restrict__ cnt, const float4* __restrict__ gv, AdamArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (a.skip_flag && *a.skip_flag) return;
+    const int ch = (int)blockIdx.y;
+    const size_t S = (size_t)n * nviews;
+    const float bc1 = a.bc_dev ? a.bc_dev[0] : a.bc1;
+    const float bc2 = a.bc_dev ? a.bc_dev[1] : a.bc2;
+    const float4 p0 = a.params[i];
+    const float pos[3] = {p0.x, p0.y, p0.z};
+    const float* mplane = reinterpret_cast<const float*>(gv + (ch == 0 ? 2 : 3) * S);
+    const int mlane = ch == 0 ? 3 : ch - 1;
+    float shg[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) shg[k] = 0.0f;
+    for (int v = 0; v < nviews; ++v) {
+        const size_t s = (size_t)v * n + i;
+        if (cnt[s] == 0) continue;
+        const float mk = mplane[s * 4 + mlane];
+        if (mk == 0.0f) continue;
+        float d[3], basis[16];
+        view_dir(pos, cams[v].pos, d);
+        sh_basis(d, basis);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) shg[k] += mk * basis[k];
+    }
+#pragma unroll
+    for (int kq = 0; kq < 4; ++kq) {
+        const int p = 3 + ch * 4 + kq;
+        const size_t o = (size_t)p * cap + i;
+        const float4 g = make_float4(shg[kq * 4 + 0], shg[kq * 4 + 1], shg[kq * 4 + 2], shg[kq * 4 + 3]);
+        a.params[o] = adam_plane(p, i, cap, a.params[o], g, a, bc1, bc2);
+    }
+}
+
 static void launch_geom_view(const float4* params, int n, int cap, const DevCam* cams, int nviews, const uint32_t* cnt,
                              const float4* acc, const float4* rec, const float4* gcache, float4* gv, cudaStream_t st) {
     size_t S = (size_t)n * nviews;
@@ -401,7 +444,7 @@ void launch_geometry_adam(const DevCam* cams, int nviews, int n, int cap, const 
                           const float4* gcache, float4* gv, const AdamArgs& a, cudaStream_t st) {
     if (n <= 0) return;
     launch_geom_view(a.params, n, cap, cams, nviews, cnt, acc, rec, gcache, gv, st);
-    k_geom_gauss<1, 1><<<(n + 127) / 128, 128, 0, st>>>(nullptr, n, cap, cams, nviews, cnt, gv, nullptr, 0, a);
+    k_geom_sh<<<dim3((unsigned)((n + 127) / 128), 3), 128, 0, st>>>(n, cap, cams, nviews, cnt, gv, a);
     k_geom_gauss<1, 2><<<(n + 127) / 128, 128, 0, st>>>(nullptr, n, cap, cams, nviews, cnt, gv, nullptr, 0, a);
 }
 
