@@ -583,7 +583,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                 pinned[v] = t
             return pinned[v]
 
-        h2d = [0]
+        h2d = [0, 0]  # bytes copied host -> device, steps
 
         def step_e2e():
             # the same view sets as the timed batched steps, so the two numbers
@@ -591,7 +591,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             views = timed_views[step_e2e.k % len(timed_views)]
             step_e2e.k += 1
             ts = [pinned_target(v) for v in views]
-            h2d[0] = sum(t.numel() * 4 for t in ts) + len(views) * 100
+            h2d[0] += sum(t.numel() * 4 for t in ts) + len(views) * 100
+            h2d[1] += 1
             if world == 1:
                 # targets copied from pinned host memory inside the step,
                 # overlapped with projection, sort and forward
@@ -606,8 +607,11 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         with torch.cuda.stream(stream):
             step_e2e()
         ke = max(3, args.steps // 2)
+        h2d[0] = h2d[1] = 0
         t_e2e = timed(step_e2e, ke)
-        e2e = {"value": world * ke / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d[0]), "d2h_bytes_per_step": 4 * V + 8}
+        # mean over the timed steps (view sets of different resolutions)
+        e2e = {"value": world * ke / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d[0] / max(h2d[1], 1)),
+               "d2h_bytes_per_step": 4 * V + 8}
 
     value = world * args.steps / t_batched
     plain_value = world * kp / t_plain
