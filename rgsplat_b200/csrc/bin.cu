@@ -40,8 +40,10 @@ __device__ __forceinline__ void bin_chunk(uint32_t n, int G, int b, uint32_t& be
 __device__ __forceinline__ uint32_t tiles_of(uint2 d) { return (d.y & 0xffffu) * (d.y >> 16); }
 
 __global__ void __launch_bounds__(BIN_THREADS) k_count_reduce(const uint32_t* __restrict__ order, const uint32_t* __restrict__ cnt,
-                                                              uint32_t S, unsigned long long* __restrict__ block_sums) {
+                                                              uint32_t S_host, const uint32_t* __restrict__ S_dev,
+                                                              unsigned long long* __restrict__ block_sums) {
     __shared__ uint32_t s_w[BIN_THREADS / 32];
+    const uint32_t S = S_dev ? *S_dev : S_host;
     uint32_t begin, end;
     bin_chunk(S, gridDim.x, blockIdx.x, begin, end);
     uint32_t s = 0;
@@ -89,9 +91,9 @@ __global__ void __launch_bounds__(1024) k_scan_block_sums(unsigned long long* __
     }
 }
 
-void launch_count_scan(const uint32_t* order, const uint32_t* cnt, uint32_t S, unsigned long long* block_sums, uint32_t* total,
-                       unsigned long long* total64, int grid, cudaStream_t st) {
-    k_count_reduce<<<grid, BIN_THREADS, 0, st>>>(order, cnt, S, block_sums);
+void launch_count_scan(const uint32_t* order, const uint32_t* cnt, uint32_t S, const uint32_t* S_dev,
+                       unsigned long long* block_sums, uint32_t* total, unsigned long long* total64, int grid, cudaStream_t st) {
+    k_count_reduce<<<grid, BIN_THREADS, 0, st>>>(order, cnt, S, S_dev, block_sums);
     k_scan_block_sums<<<1, 1024, 0, st>>>(block_sums, grid, total, total64);
 }
 
@@ -116,7 +118,8 @@ void launch_view_pairs(const uint32_t* cnt, uint32_t n, int V, unsigned long lon
     if (V > 0) k_view_pairs<<<V, BIN_THREADS, 0, st>>>(cnt, n, out);
 }
 
-__global__ void __launch_bounds__(BIN_THREADS) k_emit(const uint32_t* __restrict__ order, const uint2* __restrict__ tdesc, uint32_t S,
+__global__ void __launch_bounds__(BIN_THREADS) k_emit(const uint32_t* __restrict__ order, const uint2* __restrict__ tdesc,
+                                                      uint32_t S_host, const uint32_t* __restrict__ S_dev,
                                                       const unsigned long long* __restrict__ block_sums, uint32_t* __restrict__ pkeys,
                                                       uint32_t* __restrict__ pvals, uint32_t cap, int* __restrict__ overflow,
                                                       const uint32_t* __restrict__ total, uint32_t* __restrict__ eff,
@@ -130,7 +133,9 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit(const uint32_t* __restrict
     constexpr int PER = BIN_SUB / BIN_THREADS;
     int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     uint32_t begin, end;
-    bin_chunk(S, gridDim.x, blockIdx.x, begin, end);
+    // S_host: slots (the stride of the record planes); the order may hold fewer
+    const uint32_t S = S_host, n_order = S_dev ? *S_dev : S_host;
+    bin_chunk(n_order, gridDim.x, blockIdx.x, begin, end);
     if (blockIdx.x == 0 && threadIdx.x == 0) *eff = min(*total, cap);
     unsigned long long base = block_sums[blockIdx.x];
     for (uint32_t r0 = begin; r0 < end; r0 += BIN_SUB) {
@@ -243,7 +248,8 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit(const uint32_t* __restrict
 constexpr int EG = 4;
 __global__ void __launch_bounds__(BIN_THREADS) k_emit_pruned(const uint32_t* __restrict__ order, const uint2* __restrict__ tdesc,
                                                              const uint32_t* __restrict__ cnt, const float4* __restrict__ rec,
-                                                             uint32_t S, const unsigned long long* __restrict__ block_sums,
+                                                             uint32_t S_host, const uint32_t* __restrict__ S_dev,
+                                                             const unsigned long long* __restrict__ block_sums,
                                                              uint32_t* __restrict__ pkeys, uint32_t* __restrict__ pvals,
                                                              uint32_t cap, int* __restrict__ overflow,
                                                              const uint32_t* __restrict__ total, uint32_t* __restrict__ eff,
@@ -258,7 +264,9 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit_pruned(const uint32_t* __r
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int grp = tid / EG, gl = tid % EG;
     uint32_t begin, end;
-    bin_chunk(S, gridDim.x, blockIdx.x, begin, end);
+    // S_host: slots (the stride of the record planes); the order may hold fewer
+    const uint32_t S = S_host, n_order = S_dev ? *S_dev : S_host;
+    bin_chunk(n_order, gridDim.x, blockIdx.x, begin, end);
     if (blockIdx.x == 0 && threadIdx.x == 0) *eff = min(*total, cap);
     unsigned long long base = block_sums[blockIdx.x];
     // culled slots sort last (depth key ~0), so whole chunks of the depth
@@ -385,15 +393,91 @@ __global__ void __launch_bounds__(BIN_THREADS) k_emit_pruned(const uint32_t* __r
 }
 
 void launch_emit_pairs(const uint32_t* order, const uint2* tdesc, const uint32_t* cnt, const float4* rec, uint32_t S,
-                       const unsigned long long* block_sums, uint32_t* pair_keys, uint32_t* pair_vals, uint32_t cap, int* overflow,
-                       const uint32_t* total, const unsigned long long* total64, uint32_t* eff, const DevCam* cams,
-                       uint32_t n_per_view, int tile_w, int tile_h, int prune, int grid, cudaStream_t st) {
+                       const uint32_t* S_dev, const unsigned long long* block_sums, uint32_t* pair_keys, uint32_t* pair_vals,
+                       uint32_t cap, int* overflow, const uint32_t* total, const unsigned long long* total64, uint32_t* eff,
+                       const DevCam* cams, uint32_t n_per_view, int tile_w, int tile_h, int prune, int grid, cudaStream_t st) {
     if (prune)
-        k_emit_pruned<<<grid, BIN_THREADS, 0, st>>>(order, tdesc, cnt, rec, (uint32_t)S, block_sums, pair_keys, pair_vals, cap,
-                                                    overflow, total, eff, total64, cams, n_per_view, tile_w, tile_h);
+        k_emit_pruned<<<grid, BIN_THREADS, 0, st>>>(order, tdesc, cnt, rec, (uint32_t)S, S_dev, block_sums, pair_keys, pair_vals,
+                                                    cap, overflow, total, eff, total64, cams, n_per_view, tile_w, tile_h);
     else
-        k_emit<<<grid, BIN_THREADS, 0, st>>>(order, tdesc, S, block_sums, pair_keys, pair_vals, cap, overflow, total, eff, cams,
-                                             n_per_view);
+        k_emit<<<grid, BIN_THREADS, 0, st>>>(order, tdesc, S, S_dev, block_sums, pair_keys, pair_vals, cap, overflow, total, eff,
+                                             cams, n_per_view);
+}
+
+// ---- slots with tile pairs, compacted in slot order ------------------------
+// Before the depth sort, the slots that emit at least one pair are gathered,
+// in slot order, with their depth keys: the sort then orders only them, and
+// because it is stable and the gather keeps slot order, equal depths still
+// leave Gaussians of a view in index order. Chunks of CMP_CHUNK consecutive
+// slots: count per chunk, one exclusive scan, then a stable in-chunk scatter.
+constexpr int CMP_PER = 4;
+constexpr int CMP_CHUNK = BIN_THREADS * CMP_PER;
+
+__global__ void __launch_bounds__(BIN_THREADS) k_visible_counts(const uint32_t* __restrict__ cnt, uint32_t S,
+                                                                unsigned long long* __restrict__ chunk_counts) {
+    __shared__ uint32_t s_w[BIN_THREADS / 32];
+    const uint32_t base = blockIdx.x * (uint32_t)CMP_CHUNK + threadIdx.x * CMP_PER;
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < CMP_PER; ++k) c += (base + k < S && cnt[base + k] != 0u) ? 1u : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < BIN_THREADS / 32; ++w) t += s_w[w];
+        chunk_counts[blockIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(BIN_THREADS) k_compact_visible(const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ key,
+                                                                 uint32_t S, const unsigned long long* __restrict__ chunk_offs,
+                                                                 uint32_t* __restrict__ ckey, uint32_t* __restrict__ cslot) {
+    __shared__ uint32_t s_w[BIN_THREADS / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t base = blockIdx.x * (uint32_t)CMP_CHUNK + threadIdx.x * CMP_PER;
+    bool f[CMP_PER];
+    uint32_t local = 0;
+#pragma unroll
+    for (int k = 0; k < CMP_PER; ++k) {
+        f[k] = base + k < S && cnt[base + k] != 0u;
+        local += f[k] ? 1u : 0u;
+    }
+    uint32_t x = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_w[w] = x;
+    __syncthreads();
+    uint32_t wpre = 0;
+    for (int k = 0; k < w; ++k) wpre += s_w[k];
+    uint32_t pos = (uint32_t)chunk_offs[blockIdx.x] + wpre + x - local;
+#pragma unroll
+    for (int k = 0; k < CMP_PER; ++k) {
+        if (f[k]) {
+            ckey[pos] = key[base + k];
+            cslot[pos] = base + k;
+            ++pos;
+        }
+    }
+}
+
+size_t compact_chunks(size_t S) { return (S + CMP_CHUNK - 1) / CMP_CHUNK; }
+
+void launch_compact_visible(const uint32_t* cnt, const uint32_t* key, uint32_t S, unsigned long long* chunk_counts,
+                            uint32_t* ckey, uint32_t* cslot, uint32_t* n_out, unsigned long long* n_out64, cudaStream_t st) {
+    const unsigned chunks = (unsigned)compact_chunks(S);
+    if (chunks == 0) {
+        cudaMemsetAsync(n_out, 0, 4, st);
+        cudaMemsetAsync(n_out64, 0, 8, st);
+        return;
+    }
+    k_visible_counts<<<chunks, BIN_THREADS, 0, st>>>(cnt, S, chunk_counts);
+    k_scan_block_sums<<<1, 1024, 0, st>>>(chunk_counts, (int)chunks, n_out, n_out64);
+    k_compact_visible<<<chunks, BIN_THREADS, 0, st>>>(cnt, key, S, chunk_counts, ckey, cslot);
 }
 
 // Tile boundaries of the sorted pair keys: each thread takes four consecutive

@@ -65,7 +65,9 @@ enum {
     SC_VISIBLE = 6,
     SC_FAULT = 7,    // sticky: a sort pass's staged copies timed out
     SC_PAIRS64 = 8,  // u64 over slots 8 and 9
-    SC_COUNT = 10
+    SC_NVIS64 = 10,  // u64 over slots 10 and 11: slots with tile pairs
+    SC_NVIS = 12,    // the same, u32 (the depth sort's element count)
+    SC_COUNT = 13
 };
 
 }  // namespace
@@ -86,6 +88,7 @@ struct rgs_ctx {
     StepOut* out_h = nullptr;  // pinned
     DBuf outd;      // StepOut (device)
     DBuf rec, cnt, tdesc, dkey, ids, acc, gv;
+    DBuf ckey, cslot, chunk_counts;  // slots with tile pairs, compacted for the depth sort
     DBuf gcache;  // per-Gaussian view-independent projection terms, [2][cap] float4
     DBuf pkeys, pvals;
     uint32_t pair_cap = 0;
@@ -363,6 +366,9 @@ int ensure_work(rgs_ctx* ctx, size_t S, size_t px, size_t tiles, size_t lblocks,
     CK(ctx->tdesc.ensure(std::max<size_t>(S, 1) * 8));
     CK(ctx->dkey.ensure(std::max<size_t>(S, 1) * 4));
     CK(ctx->ids.ensure(std::max<size_t>(S, 1) * 4));
+    CK(ctx->ckey.ensure(std::max<size_t>(S, 1) * 4));
+    CK(ctx->cslot.ensure(std::max<size_t>(S, 1) * 4));
+    CK(ctx->chunk_counts.ensure(std::max<size_t>(compact_chunks(S), 1) * 8));
     CK(ctx->ranges.ensure(std::max<size_t>(tiles, 1) * sizeof(uint2)));
     CK(ctx->rgb.ensure(px * 3 * 4));
     CK(ctx->final_t.ensure(px * 4));
@@ -423,14 +429,20 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
                        ctx->ids.as<uint32_t>(), prune ? 1 : 0, sc + SC_VISIBLE, ctx->gcache.as<float4>(), st);
     }
     mark(ctx, 1);
+    // only the slots with tile pairs go through the depth sort, gathered in
+    // slot order (the stable sort then still breaks depth ties by index)
+    launch_compact_visible(ctx->cnt.as<uint32_t>(), ctx->dkey.as<uint32_t>(), (uint32_t)S,
+                           ctx->chunk_counts.as<unsigned long long>(), ctx->ckey.as<uint32_t>(), ctx->cslot.as<uint32_t>(),
+                           sc + SC_NVIS, (unsigned long long*)(sc + SC_NVIS64), st);
+    const uint32_t* nvis = sc + SC_NVIS;
     cudaError_t e;
-    int which = radix_sort_pairs(ctx->dkey.as<uint32_t>(), ctx->ids.as<uint32_t>(), (uint32_t)S, nullptr, 32, ctx->sort,
+    int which = radix_sort_pairs(ctx->ckey.as<uint32_t>(), ctx->cslot.as<uint32_t>(), (uint32_t)S, nvis, 32, ctx->sort,
                                  ctx->sort_grid, st, &e);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "depth sort");
     mark(ctx, 2);
-    const uint32_t* order = which ? ctx->sort.vals2.as<uint32_t>() : ctx->ids.as<uint32_t>();
-    launch_count_scan(order, ctx->cnt.as<uint32_t>(), (uint32_t)S, ctx->block_sums.as<unsigned long long>(), sc + SC_PAIRS,
-                      (unsigned long long*)(sc + SC_PAIRS64), bin_grid_blocks(), st);
+    const uint32_t* order = which ? ctx->sort.vals2.as<uint32_t>() : ctx->cslot.as<uint32_t>();
+    launch_count_scan(order, ctx->cnt.as<uint32_t>(), (uint32_t)S, nvis, ctx->block_sums.as<unsigned long long>(),
+                      sc + SC_PAIRS, (unsigned long long*)(sc + SC_PAIRS64), bin_grid_blocks(), st);
     if (host_count) {
         unsigned long long K = 0;
         uint32_t vis = 0;
@@ -464,7 +476,7 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
         }
     }
     CK(cudaMemsetAsync(sc + SC_OVERFLOW, 0, 4, st));
-    launch_emit_pairs(order, ctx->tdesc.as<uint2>(), ctx->cnt.as<uint32_t>(), ctx->rec.as<float4>(), (uint32_t)S,
+    launch_emit_pairs(order, ctx->tdesc.as<uint2>(), ctx->cnt.as<uint32_t>(), ctx->rec.as<float4>(), (uint32_t)S, nvis,
                       ctx->block_sums.as<unsigned long long>(), ctx->pkeys.as<uint32_t>(), ctx->pvals.as<uint32_t>(), ctx->pair_cap,
                       (int*)(sc + SC_OVERFLOW), sc + SC_PAIRS, (const unsigned long long*)(sc + SC_PAIRS64), sc + SC_PAIRS_EFF,
                       cams_dev, (uint32_t)s.n, ctx->opt.tile_w,
@@ -723,7 +735,8 @@ void rgs_destroy(rgs_ctx* ctx) {
         s->params.release(); s->grads.release(); s->m1.release(); s->m2.release(); s->accum.release(); s->denom.release();
     }
     for (auto& t : ctx->targets) t.release();
-    DBuf* bufs[] = {&ctx->hdr, &ctx->outd, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->gcache, &ctx->dkey, &ctx->ids, &ctx->acc, &ctx->gv, &ctx->pkeys, &ctx->pvals,
+    DBuf* bufs[] = {&ctx->hdr, &ctx->outd, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->gcache, &ctx->dkey, &ctx->ids,
+                    &ctx->ckey, &ctx->cslot, &ctx->chunk_counts, &ctx->acc, &ctx->gv, &ctx->pkeys, &ctx->pvals,
                     &ctx->ranges, &ctx->rgb, &ctx->final_t, &ctx->last, &ctx->dl, &ctx->partials, &ctx->scalars,
                     &ctx->block_sums, &ctx->view_pairs, &ctx->sort.hist, &ctx->sort.keys2, &ctx->sort.vals2, &ctx->dens_scratch,
                     &ctx->dens_out, &ctx->m_tmp, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->stage_d,
@@ -1496,7 +1509,8 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
         // Everything a captured graph bakes in: sizes, every buffer address, and
         // the loss weight, background and optimiser constants.
         const DBuf* bufs[] = {&s.params, &s.grads, &s.m1, &s.m2, &s.accum, &s.denom, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->gv, &ctx->gcache, &ctx->dkey,
-                              &ctx->ids, &ctx->acc, &ctx->pkeys, &ctx->pvals, &ctx->ranges, &ctx->rgb, &ctx->final_t,
+                              &ctx->ids, &ctx->ckey, &ctx->cslot, &ctx->chunk_counts, &ctx->acc, &ctx->pkeys,
+                              &ctx->pvals, &ctx->ranges, &ctx->rgb, &ctx->final_t,
                               &ctx->last, &ctx->dl, &ctx->partials, &ctx->scalars, &ctx->block_sums, &ctx->hdr, &ctx->outd,
                               &ctx->sort.hist, &ctx->sort.keys2, &ctx->sort.vals2};
         float fk[14] = {bg[0], bg[1], bg[2], lambda, tc.lr_position, tc.lr_rotation, tc.lr_scale, tc.lr_opacity,

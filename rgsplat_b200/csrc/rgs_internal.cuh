@@ -184,15 +184,22 @@ inline size_t sort_hist_bytes(int grid) { return ((size_t)grid * 256 + 256) * 4;
 // expands only the tiles of each row's kept span, recomputed from the record.
 // block_sums: one u64 per CTA of `grid`; *total is the pair count saturated
 // at 2^32 - 1, *total64 the exact count.
-void launch_count_scan(const uint32_t* order, const uint32_t* cnt, uint32_t S, unsigned long long* block_sums,
-                       uint32_t* total, unsigned long long* total64, int grid, cudaStream_t st);
+// S_dev (may be null) holds the number of order entries on the device.
+void launch_count_scan(const uint32_t* order, const uint32_t* cnt, uint32_t S, const uint32_t* S_dev,
+                       unsigned long long* block_sums, uint32_t* total, unsigned long long* total64, int grid, cudaStream_t st);
 // Per-view pair totals (slot = view * n + Gaussian) into out[0, V).
 void launch_view_pairs(const uint32_t* cnt, uint32_t n, int V, unsigned long long* out, cudaStream_t st);
 void launch_emit_pairs(const uint32_t* order, const uint2* tdesc, const uint32_t* cnt, const float4* rec, uint32_t S,
-                       const unsigned long long* block_sums, uint32_t* pair_keys, uint32_t* pair_vals, uint32_t cap, int* overflow,
-                       const uint32_t* total, const unsigned long long* total64, uint32_t* eff, const DevCam* cams,
-                       uint32_t n_per_view, int tile_w, int tile_h, int prune, int grid, cudaStream_t st);
+                       const uint32_t* S_dev, const unsigned long long* block_sums, uint32_t* pair_keys, uint32_t* pair_vals,
+                       uint32_t cap, int* overflow, const uint32_t* total, const unsigned long long* total64, uint32_t* eff,
+                       const DevCam* cams, uint32_t n_per_view, int tile_w, int tile_h, int prune, int grid, cudaStream_t st);
 int bin_grid_blocks();
+// The slots with at least one tile pair (cnt != 0), gathered in slot order:
+// their keys into ckey, their slot indices into cslot, the count into *n_out
+// (and *n_out64). chunk_counts holds compact_chunks(S) u64.
+size_t compact_chunks(size_t S);
+void launch_compact_visible(const uint32_t* cnt, const uint32_t* key, uint32_t S, unsigned long long* chunk_counts,
+                            uint32_t* ckey, uint32_t* cslot, uint32_t* n_out, unsigned long long* n_out64, cudaStream_t st);
 void launch_tile_ranges(const uint32_t* pair_keys, const uint32_t* total, uint32_t cap, uint2* ranges,
                         cudaStream_t st);
 
