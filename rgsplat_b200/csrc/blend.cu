@@ -501,8 +501,9 @@ __global__ void __launch_bounds__(TW * TH / PPT, PPT == 2 ? 8 : PPT == 4 ? 12 : 
                             const float2 al = make_float2(a0 ? al0 : 0.0f, a1 ? al1 : 0.0f);
                             const float2 om = __ffma2_rn(al, bc2(-1.0f), bc2(1.0f));
                             const float2 inv = make_float2(__fdividef(1.0f, om.x), __fdividef(1.0f, om.y));
-                            float2 Tp = __fmul2_rn(make_float2(T[p0], T[p1]), inv);
-                            Tp = make_float2(a0 ? Tp.x : T[p0], a1 ? Tp.y : T[p1]);
+                            // a lane with alpha = 0 has 1 - alpha = 1 and rcp(1) = 1, so its
+                            // T is multiplied by exactly 1
+                            const float2 Tp = __fmul2_rn(make_float2(T[p0], T[p1]), inv);
                             T[p0] = Tp.x;
                             T[p1] = Tp.y;
                             const float2 w = __fmul2_rn(al, Tp);
@@ -521,8 +522,10 @@ __global__ void __launch_bounds__(TW * TH / PPT, PPT == 2 ? 8 : PPT == 4 ? 12 : 
                             // zero for a lane that does not take the splat or whose raw
                             // alpha was clamped (backward.rs:459-461)
                             const float2 draw = make_float2(a0 && !(ar.x > 0.99f) ? dda.x : 0.0f, a1 && !(ar.y > 0.99f) ? dda.y : 0.0f);
-                            G3 = __ffma2_rn(draw, make_float2(a0 ? ge.x : 0.0f, a1 ? ge.y : 0.0f), G3);
-                            const float2 u = __fmul2_rn(draw, make_float2(a0 ? ar.x : 0.0f, a1 ? ar.y : 0.0f));
+                            // every lane's exp and raw alpha are finite (power <= 0 up to
+                            // rounding), so a zero draw zeroes its terms
+                            G3 = __ffma2_rn(draw, ge, G3);
+                            const float2 u = __fmul2_rn(draw, ar);
                             SU = __fadd2_rn(SU, u);
                             SUD = __ffma2_rn(u, dy2, SUD);
                             SUDD = __ffma2_rn(__fmul2_rn(u, dy2), dy2, SUDD);
