@@ -35,7 +35,8 @@ struct StepHdr {
     uint32_t total_tiles;
     uint32_t total_loss_blocks;
     float bc[2];
-    uint32_t pad[4];
+    uint32_t total_st;   // supertiles of the batch
+    uint32_t pad[3];
     DevCam cams[MAX_VIEWS];
 };
 
@@ -46,6 +47,7 @@ struct StepOut {
     uint32_t pad;
     float losses[MAX_VIEWS];
     unsigned long long pairs64;  // exact pair count (pairs saturates at 2^32 - 1)
+    unsigned long long st_pairs64;  // (supertile, slot) entries of the batch
     int sort_fault;
     int pad2;
 };
@@ -57,7 +59,6 @@ constexpr unsigned long long BATCH_PAIR_LIMIT = 1ull << 30;
 
 enum {
     SC_PAIRS = 0,
-    SC_PAIRS_EFF = 1,
     SC_OVERFLOW = 2,
     SC_WORK_F = 3,
     SC_WORK_B = 4,
@@ -67,7 +68,10 @@ enum {
     SC_PAIRS64 = 8,  // u64 over slots 8 and 9
     SC_NVIS64 = 10,  // u64 over slots 10 and 11: slots with tile pairs
     SC_NVIS = 12,    // the same, u32 (the depth sort's element count)
-    SC_COUNT = 13
+    SC_STPAIRS64 = 14,  // u64 over 14 and 15: (supertile, slot) entries
+    SC_STPAIRS = 16,    // the same, saturated u32
+    SC_STEFF = 17,      // entries held (the supertile sort's element count)
+    SC_COUNT = 18
 };
 
 }  // namespace
@@ -89,6 +93,10 @@ struct rgs_ctx {
     DBuf outd;      // StepOut (device)
     DBuf rec, cnt, tdesc, dkey, ids, acc, gv;
     DBuf ckey, cslot, chunk_counts;  // slots with tile pairs, compacted for the depth sort
+    // supertile binning: per slot the supertile count and rectangle, per
+    // entry the tile mask, per chunk of entries and tile position the counts,
+    // per position the total, and the count scan's block sums
+    DBuf st_cnt, st_desc, st_masks, st_chunks, st_planes, st_block_sums;
     DBuf gcache;  // per-Gaussian view-independent projection terms, [2][cap] float4
     DBuf pkeys, pvals;
     uint32_t pair_cap = 0;
@@ -209,6 +217,8 @@ int make_devcam(rgs_ctx* ctx, const rgs_camera& c, DevCam& d) {
     d.ref_tiles_y = (d.height + REF_TILE - 1) / REF_TILE;
     d.tiles_x = (d.width + ctx->opt.tile_w - 1) / ctx->opt.tile_w;
     d.tiles_y = (d.height + ctx->opt.tile_h - 1) / ctx->opt.tile_h;
+    d.st_x = (d.tiles_x + ST_EDGE - 1) / ST_EDGE;
+    d.st_base = 0;
     d.loss_bx = (d.width + LOSS_TILE - 1) / LOSS_TILE;
     d.tile_base = d.pix_base = d.loss_base = 0;
     d.target = nullptr;
@@ -216,9 +226,19 @@ int make_devcam(rgs_ctx* ctx, const rgs_camera& c, DevCam& d) {
 }
 
 // Lays out V views in one batch; returns (pixels, tiles, loss blocks).
+// Supertiles of a batch whose views' st_base are assigned.
+size_t batch_supertiles(const DevCam* d, int V) {
+    if (V <= 0) return 0;
+    const DevCam& c = d[V - 1];
+    return (size_t)c.st_base + (size_t)c.st_x * ((c.tiles_y + ST_EDGE - 1) / ST_EDGE);
+}
+
 void assign_bases(DevCam* d, int V, size_t& px, size_t& tiles, size_t& lblocks) {
     px = tiles = lblocks = 0;
+    size_t sts = 0;
     for (int v = 0; v < V; ++v) {
+        d[v].st_base = (int)sts;
+        sts += (size_t)d[v].st_x * ((d[v].tiles_y + ST_EDGE - 1) / ST_EDGE);
         d[v].tile_base = (int)tiles;
         d[v].pix_base = (int)px;
         d[v].loss_base = (int)lblocks;
@@ -369,6 +389,10 @@ int ensure_work(rgs_ctx* ctx, size_t S, size_t px, size_t tiles, size_t lblocks,
     CK(ctx->ckey.ensure(std::max<size_t>(S, 1) * 4));
     CK(ctx->cslot.ensure(std::max<size_t>(S, 1) * 4));
     CK(ctx->chunk_counts.ensure(std::max<size_t>(compact_chunks(S), 1) * 8));
+    CK(ctx->st_cnt.ensure(std::max<size_t>(S, 1) * 4));
+    CK(ctx->st_desc.ensure(std::max<size_t>(S, 1) * 8));
+    CK(ctx->st_planes.ensure(ST_TILES * 4));
+    CK(ctx->st_block_sums.ensure((size_t)bin_grid_blocks() * 8 + 64));
     CK(ctx->ranges.ensure(std::max<size_t>(tiles, 1) * sizeof(uint2)));
     CK(ctx->rgb.ensure(px * 3 * 4));
     CK(ctx->final_t.ensure(px * 4));
@@ -400,8 +424,12 @@ int ensure_pairs(rgs_ctx* ctx, unsigned long long K) {
     cap = std::min<unsigned long long>(cap, 0xF0000000ull);
     ctx->pkeys.release();
     ctx->pvals.release();
+    ctx->st_masks.release();
+    ctx->st_chunks.release();
     CK(ctx->pkeys.ensure(cap * 4));
     CK(ctx->pvals.ensure(cap * 4));
+    CK(ctx->st_masks.ensure(cap * 2));
+    CK(ctx->st_chunks.ensure(supertile_chunks(cap) * ST_TILES * 4));
     ctx->pair_cap = (uint32_t)cap;
     return RGS_OK;
 }
@@ -418,7 +446,10 @@ struct Binned {
 // Only valid with a zero background, where a pixel whose reference tile list
 // is empty renders the same 0 as one whose splats all miss it.
 int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tiles, bool host_count, Binned& out,
-              bool project = true, bool prune = false) {
+              bool project = true, bool prune = false, size_t st_cap = 0) {
+    // supertiles the buffers and scans cover: the batch's own unless the
+    // caller (a captured graph replayed for other views) gives a bound
+    if (!st_cap) st_cap = std::max<size_t>(ctx->hdr_h->total_st, 1);
     cudaStream_t st = ctx->st;
     const size_t S = (size_t)s.n * V;
     uint32_t* sc = ctx->scalars.as<uint32_t>();
@@ -430,10 +461,12 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
     }
     mark(ctx, 1);
     // only the slots with tile pairs go through the depth sort, gathered in
-    // slot order (the stable sort then still breaks depth ties by index)
+    // slot order (the stable sort then still breaks depth ties by index);
+    // the gather also writes each slot's supertile rectangle and count
     launch_compact_visible(ctx->cnt.as<uint32_t>(), ctx->dkey.as<uint32_t>(), (uint32_t)S,
                            ctx->chunk_counts.as<unsigned long long>(), ctx->ckey.as<uint32_t>(), ctx->cslot.as<uint32_t>(),
-                           sc + SC_NVIS, (unsigned long long*)(sc + SC_NVIS64), st);
+                           sc + SC_NVIS, (unsigned long long*)(sc + SC_NVIS64), ctx->tdesc.as<uint2>(), cams_dev,
+                           (uint32_t)s.n, ctx->st_cnt.as<uint32_t>(), ctx->st_desc.as<uint2>(), st);
     const uint32_t* nvis = sc + SC_NVIS;
     cudaError_t e;
     int which = radix_sort_pairs(ctx->ckey.as<uint32_t>(), ctx->cslot.as<uint32_t>(), (uint32_t)S, nvis, 32, ctx->sort,
@@ -441,23 +474,28 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
     if (e != cudaSuccess) return cuda_fail(ctx, e, "depth sort");
     mark(ctx, 2);
     const uint32_t* order = which ? ctx->sort.vals2.as<uint32_t>() : ctx->cslot.as<uint32_t>();
+    // (tile, slot) pairs of the batch, and (supertile, slot) entries
     launch_count_scan(order, ctx->cnt.as<uint32_t>(), (uint32_t)S, nvis, ctx->block_sums.as<unsigned long long>(),
                       sc + SC_PAIRS, (unsigned long long*)(sc + SC_PAIRS64), bin_grid_blocks(), st);
+    launch_count_scan(order, ctx->st_cnt.as<uint32_t>(), (uint32_t)S, nvis, ctx->st_block_sums.as<unsigned long long>(),
+                      sc + SC_STPAIRS, (unsigned long long*)(sc + SC_STPAIRS64), bin_grid_blocks(), st);
     if (host_count) {
-        unsigned long long K = 0;
+        unsigned long long K = 0, KS = 0;
         uint32_t vis = 0;
         int fault = 0;
         CK(cudaMemcpyAsync(&K, sc + SC_PAIRS64, 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&KS, sc + SC_STPAIRS64, 8, cudaMemcpyDeviceToHost, st));
         if (project) CK(cudaMemcpyAsync(&vis, sc + SC_VISIBLE, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(&fault, sc + SC_FAULT, 4, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         if (fault) return fail(ctx, RGS_ERR_CUDA, "a sort pass's staged copies timed out");
         ctx->stats.visible += vis;
-        int rc = ensure_pairs(ctx, K);
+        int rc = ensure_pairs(ctx, std::max(K, KS));
         if (rc) return rc;
         ctx->stats.pairs += K;
-        // the depth order may live in the sort scratch: size it for the tile
-        // sort now, while nothing is in flight, so the tile sort never reallocates it
+        // the depth order may live in the sort scratch: size it for the
+        // supertile sort now, while nothing is in flight, so that sort never
+        // reallocates it
         size_t need = std::max<size_t>(S, ctx->pair_cap) * 4 + 16;
         if (ctx->sort.keys2.bytes < need || ctx->sort.vals2.bytes < need) {
             std::vector<uint32_t> tmp;
@@ -476,22 +514,44 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
         }
     }
     CK(cudaMemsetAsync(sc + SC_OVERFLOW, 0, 4, st));
-    launch_emit_pairs(order, ctx->tdesc.as<uint2>(), ctx->cnt.as<uint32_t>(), ctx->rec.as<float4>(), (uint32_t)S, nvis,
-                      ctx->block_sums.as<unsigned long long>(), ctx->pkeys.as<uint32_t>(), ctx->pvals.as<uint32_t>(), ctx->pair_cap,
-                      (int*)(sc + SC_OVERFLOW), sc + SC_PAIRS, (const unsigned long long*)(sc + SC_PAIRS64), sc + SC_PAIRS_EFF,
-                      cams_dev, (uint32_t)s.n, ctx->opt.tile_w,
-                      ctx->opt.tile_h, prune ? 1 : 0, bin_grid_blocks(), st);
+    launch_emit_supertiles(order, ctx->st_desc.as<uint2>(), (uint32_t)S, nvis, ctx->st_block_sums.as<unsigned long long>(),
+                           ctx->pkeys.as<uint32_t>(), ctx->pvals.as<uint32_t>(), ctx->pair_cap, (int*)(sc + SC_OVERFLOW),
+                           sc + SC_STPAIRS, sc + SC_STEFF, cams_dev, (uint32_t)s.n, bin_grid_blocks(), st);
     mark(ctx, 3);
-    int which2 = radix_sort_pairs(ctx->pkeys.as<uint32_t>(), ctx->pvals.as<uint32_t>(), ctx->pair_cap, sc + SC_PAIRS_EFF,
-                                  bits_for(std::max<size_t>(tiles, 2)), ctx->sort, ctx->sort_grid, st, &e);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "tile sort");
+    int which2 = radix_sort_pairs(ctx->pkeys.as<uint32_t>(), ctx->pvals.as<uint32_t>(), ctx->pair_cap, sc + SC_STEFF,
+                                  bits_for(std::max<size_t>(st_cap, 2)), ctx->sort, ctx->sort_grid, st, &e);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "supertile sort");
     mark(ctx, 4);
-    out.keys = which2 ? ctx->sort.keys2.as<uint32_t>() : ctx->pkeys.as<uint32_t>();
-    out.vals = which2 ? ctx->sort.vals2.as<uint32_t>() : ctx->pvals.as<uint32_t>();
+    const uint32_t* ent_keys = which2 ? ctx->sort.keys2.as<uint32_t>() : ctx->pkeys.as<uint32_t>();
+    const uint32_t* ent_slot = which2 ? ctx->sort.vals2.as<uint32_t>() : ctx->pvals.as<uint32_t>();
+    uint32_t* lists = which2 ? ctx->pvals.as<uint32_t>() : ctx->sort.vals2.as<uint32_t>();
+    // tiles no entry's supertile holds keep an empty range
     CK(cudaMemsetAsync(ctx->ranges.p, 0, std::max<size_t>(tiles, 1) * sizeof(uint2), st));
-    launch_tile_ranges(out.keys, sc + SC_PAIRS, ctx->pair_cap, ctx->ranges.as<uint2>(), st);
+    SupertileArgs sa;
+    sa.cams = cams_dev;
+    sa.nviews = V;
+    sa.ent_key = ent_keys;
+    sa.ent_slot = ent_slot;
+    sa.n_ent = sc + SC_STEFF;
+    sa.tdesc = ctx->tdesc.as<uint2>();
+    sa.rec = ctx->rec.as<float4>();
+    sa.S = (uint32_t)S;
+    sa.tile_w = ctx->opt.tile_w;
+    sa.tile_h = ctx->opt.tile_h;
+    sa.prune = prune ? 1 : 0;
+    sa.masks = ctx->st_masks.as<uint16_t>();
+    sa.chunk_cnt = ctx->st_chunks.as<uint32_t>();
+    sa.chunk_stride = (uint32_t)supertile_chunks(ctx->pair_cap);
+    sa.plane_tot = ctx->st_planes.as<uint32_t>();
+    sa.vals_out = lists;
+    sa.cap = ctx->pair_cap;
+    sa.ranges = ctx->ranges.as<uint2>();
+    sa.overflow = (int*)(sc + SC_OVERFLOW);
+    launch_supertile_lists(sa, st);
     mark(ctx, 5);
     CK(cudaGetLastError());
+    out.keys = nullptr;
+    out.vals = lists;
     return RGS_OK;
 }
 
@@ -530,6 +590,7 @@ int upload_single_cam(rgs_ctx* ctx, const DevCam& d, DevCam** dev) {
     h->cams[0] = d;
     h->total_tiles = (uint32_t)(d.tiles_x * d.tiles_y);
     h->total_loss_blocks = (uint32_t)(d.loss_bx * ((d.height + LOSS_TILE - 1) / LOSS_TILE));
+    h->total_st = (uint32_t)batch_supertiles(&d, 1);
     CK(cudaMemcpyAsync(ctx->hdr.p, h, sizeof(StepHdr), cudaMemcpyHostToDevice, ctx->st));
     *dev = (DevCam*)((char*)ctx->hdr.p + offsetof(StepHdr, cams));
     // the host header is reused by the next call: wait for the copy
@@ -736,7 +797,9 @@ void rgs_destroy(rgs_ctx* ctx) {
     }
     for (auto& t : ctx->targets) t.release();
     DBuf* bufs[] = {&ctx->hdr, &ctx->outd, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->gcache, &ctx->dkey, &ctx->ids,
-                    &ctx->ckey, &ctx->cslot, &ctx->chunk_counts, &ctx->acc, &ctx->gv, &ctx->pkeys, &ctx->pvals,
+                    &ctx->ckey, &ctx->cslot, &ctx->chunk_counts, &ctx->st_cnt, &ctx->st_desc, &ctx->st_masks,
+                    &ctx->st_chunks, &ctx->st_planes, &ctx->st_block_sums, &ctx->acc, &ctx->gv, &ctx->pkeys,
+                    &ctx->pvals,
                     &ctx->ranges, &ctx->rgb, &ctx->final_t, &ctx->last, &ctx->dl, &ctx->partials, &ctx->scalars,
                     &ctx->block_sums, &ctx->view_pairs, &ctx->sort.hist, &ctx->sort.keys2, &ctx->sort.vals2, &ctx->dens_scratch,
                     &ctx->dens_out, &ctx->m_tmp, &ctx->stage_a, &ctx->stage_b, &ctx->stage_c, &ctx->stage_d,
@@ -1392,7 +1455,13 @@ int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], fl
     cudaMemcpyAsync(ctx->hdr.p, ctx->hdr_h, sizeof(StepHdr), cudaMemcpyHostToDevice, st);
     mark(ctx, 0);
     Binned b;
-    int rc = bin_batch(ctx, s, cams_dev, V, tiles_cap, false, b, true, zero_bg(bg));
+    // supertiles of any V views of this context (the graph is replayed for other view sets)
+    size_t st_view_max = 1;
+    for (const rgs_camera& cam : ctx->cams) {
+        const size_t tx = (cam.width + ctx->opt.tile_w - 1) / ctx->opt.tile_w, ty = (cam.height + ctx->opt.tile_h - 1) / ctx->opt.tile_h;
+        st_view_max = std::max(st_view_max, ((tx + ST_EDGE - 1) / ST_EDGE) * ((ty + ST_EDGE - 1) / ST_EDGE));
+    }
+    int rc = bin_batch(ctx, s, cams_dev, V, tiles_cap, false, b, true, zero_bg(bg), st_view_max * (size_t)V);
     if (!rc) {
         BlendArgs fa = blend_args(ctx, s, cams_dev, V, &hd->total_tiles, tiles_cap, b, bg, true);
         launch_blend_forward(fa, ctx->opt.tile_w, ctx->opt.tile_h, ctx->opt.batch, st);
@@ -1424,6 +1493,7 @@ int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], fl
         mark(ctx, 9);
         cudaMemcpyAsync(&ctx->out_h->pairs, sc + SC_PAIRS, 4, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(&ctx->out_h->pairs64, sc + SC_PAIRS64, 8, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(&ctx->out_h->st_pairs64, sc + SC_STPAIRS64, 8, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(&ctx->out_h->sort_fault, sc + SC_FAULT, 4, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(&ctx->out_h->overflow, sc + SC_OVERFLOW, 4, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(&ctx->out_h->visible, sc + SC_VISIBLE, 4, cudaMemcpyDeviceToHost, st);
@@ -1462,6 +1532,7 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
     assign_bases(h->cams, V, px, tiles, lb);
     h->total_tiles = (uint32_t)tiles;
     h->total_loss_blocks = (uint32_t)lb;
+    h->total_st = (uint32_t)batch_supertiles(h->cams, V);
     size_t px_cap, tiles_cap, lb_cap;
     batch_caps(ctx, V, px_cap, tiles_cap, lb_cap);
     size_t S = (size_t)s.n * V;
@@ -1509,7 +1580,9 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
         // Everything a captured graph bakes in: sizes, every buffer address, and
         // the loss weight, background and optimiser constants.
         const DBuf* bufs[] = {&s.params, &s.grads, &s.m1, &s.m2, &s.accum, &s.denom, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->gv, &ctx->gcache, &ctx->dkey,
-                              &ctx->ids, &ctx->ckey, &ctx->cslot, &ctx->chunk_counts, &ctx->acc, &ctx->pkeys,
+                              &ctx->ids, &ctx->ckey, &ctx->cslot, &ctx->chunk_counts, &ctx->st_cnt, &ctx->st_desc,
+                              &ctx->st_masks, &ctx->st_chunks, &ctx->st_planes, &ctx->st_block_sums,
+                              &ctx->acc, &ctx->pkeys,
                               &ctx->pvals, &ctx->ranges, &ctx->rgb, &ctx->final_t,
                               &ctx->last, &ctx->dl, &ctx->partials, &ctx->scalars, &ctx->block_sums, &ctx->hdr, &ctx->outd,
                               &ctx->sort.hist, &ctx->sort.keys2, &ctx->sort.vals2};
@@ -1570,7 +1643,8 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
         if (accumulate) return fail(ctx, RGS_ERR_CAPACITY, "a view group outgrew its pair buffer");
         const unsigned long long K = ctx->out_h->pairs64;
         if (K > ctx->opt.batch_pair_limit && allow_split && V > 1) return split_step(ctx, views, V, bg, lambda, tc, losses, fused, host_targets);
-        if ((rc = ensure_pairs(ctx, K))) return rc;
+        // the supertile entries share the pair buffers: room for both
+        if ((rc = ensure_pairs(ctx, std::max(K, (unsigned long long)ctx->out_h->st_pairs64)))) return rc;
     }
     return fail(ctx, RGS_ERR_CAPACITY, "pair buffer overflow persisted");
 }
@@ -2098,22 +2172,22 @@ int rgs_debug_tile_lists(rgs_ctx* ctx, const float* gaussians, size_t n, const r
     *n_pairs = K;
     if (!entries) return RGS_OK;
     if (!offsets || cap < K) return fail(ctx, RGS_ERR_CAPACITY, "entries buffer too small");
-    std::vector<uint32_t> keys(K), vals(K);
-    if (K) {
-        CK(cudaMemcpyAsync(keys.data(), b.keys, (size_t)K * 4, cudaMemcpyDeviceToHost, ctx->st));
-        CK(cudaMemcpyAsync(vals.data(), b.vals, (size_t)K * 4, cudaMemcpyDeviceToHost, ctx->st));
-        CK(cudaStreamSynchronize(ctx->st));
-    }
+    // each tile's list is ranges[t] in the list buffer (lists are grouped by
+    // supertile there): concatenate them in tile order
+    std::vector<uint2> rg(std::max<size_t>(tiles, 1));
+    std::vector<uint32_t> vals(std::max<uint32_t>(K, 1));
+    CK(cudaMemcpyAsync(rg.data(), ctx->ranges.p, tiles * sizeof(uint2), cudaMemcpyDeviceToHost, ctx->st));
+    if (K) CK(cudaMemcpyAsync(vals.data(), b.vals, (size_t)K * 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
     size_t k = 0;
     for (size_t t = 0; t < tiles; ++t) {
         offsets[t] = (int32_t)k;
-        while (k < K && keys[k] == t) {
-            entries[k] = (int32_t)vals[k];
-            ++k;
-        }
+        if (rg[t].y < rg[t].x || rg[t].y > K || k + (rg[t].y - rg[t].x) > K)
+            return fail(ctx, RGS_ERR_CUDA, "internal: tile ranges out of bounds");
+        for (uint32_t p = rg[t].x; p < rg[t].y; ++p) entries[k++] = (int32_t)vals[p];
     }
     offsets[tiles] = (int32_t)k;
-    if (k != K) return fail(ctx, RGS_ERR_CUDA, "internal: pair keys out of order");
+    if (k != K) return fail(ctx, RGS_ERR_CUDA, "internal: tile lists do not hold every pair");
     return RGS_OK;
 }
 

@@ -45,8 +45,16 @@ struct DevCam {
     int pix_base;              // first pixel of this view in the batch buffers
     int loss_base;             // first loss block of this view
     int loss_bx;               // loss blocks per row
+    int st_x;                  // supertiles (4x4 CTA tiles) per row
+    int st_base;               // first global supertile of this view
     const float* target;       // RGBA float target (w*h*4), device
 };
+
+// Tile lists are built through supertiles of ST_EDGE x ST_EDGE CTA tiles: the
+// slots are first sorted by supertile, then the sorted entries are expanded
+// into the lists of the supertiles' tiles (supertile.cu).
+constexpr int ST_EDGE = 4;
+constexpr int ST_TILES = ST_EDGE * ST_EDGE;
 
 // Reference record (Gaussian3D) float index -> (plane, lane).
 __host__ __device__ inline void record_to_plane(int f, int& p, int& l) {
@@ -180,28 +188,56 @@ int sort_grid_blocks();
 inline size_t sort_hist_bytes(int grid) { return ((size_t)grid * 256 + 256) * 4; }
 
 // bin.cu
-// Pair counts come from cnt[] (full or pruned); with prune the emission
-// expands only the tiles of each row's kept span, recomputed from the record.
-// block_sums: one u64 per CTA of `grid`; *total is the pair count saturated
-// at 2^32 - 1, *total64 the exact count.
+// Exclusive scan of the per-slot counts cnt[order[r]] in depth order (pruned
+// tile pairs, or supertile entries). block_sums: one u64 per CTA of `grid`;
+// *total is the count saturated at 2^32 - 1, *total64 the exact count.
 // S_dev (may be null) holds the number of order entries on the device.
 void launch_count_scan(const uint32_t* order, const uint32_t* cnt, uint32_t S, const uint32_t* S_dev,
                        unsigned long long* block_sums, uint32_t* total, unsigned long long* total64, int grid, cudaStream_t st);
 // Per-view pair totals (slot = view * n + Gaussian) into out[0, V).
 void launch_view_pairs(const uint32_t* cnt, uint32_t n, int V, unsigned long long* out, cudaStream_t st);
-void launch_emit_pairs(const uint32_t* order, const uint2* tdesc, const uint32_t* cnt, const float4* rec, uint32_t S,
-                       const uint32_t* S_dev, const unsigned long long* block_sums, uint32_t* pair_keys, uint32_t* pair_vals,
-                       uint32_t cap, int* overflow, const uint32_t* total, const unsigned long long* total64, uint32_t* eff,
-                       const DevCam* cams, uint32_t n_per_view, int tile_w, int tile_h, int prune, int grid, cudaStream_t st);
 int bin_grid_blocks();
 // The slots with at least one tile pair (cnt != 0), gathered in slot order:
 // their keys into ckey, their slot indices into cslot, the count into *n_out
 // (and *n_out64). chunk_counts holds compact_chunks(S) u64.
 size_t compact_chunks(size_t S);
 void launch_compact_visible(const uint32_t* cnt, const uint32_t* key, uint32_t S, unsigned long long* chunk_counts,
-                            uint32_t* ckey, uint32_t* cslot, uint32_t* n_out, unsigned long long* n_out64, cudaStream_t st);
-void launch_tile_ranges(const uint32_t* pair_keys, const uint32_t* total, uint32_t cap, uint2* ranges,
-                        cudaStream_t st);
+                            uint32_t* ckey, uint32_t* cslot, uint32_t* n_out, unsigned long long* n_out64,
+                            const uint2* tdesc, const DevCam* cams, uint32_t n_per_view, uint32_t* st_cnt, uint2* st_desc,
+                            cudaStream_t st);
+// Supertile rectangles expanded into (supertile id, slot) entries in the
+// order's (depth) order: the rectangle emitter with the view's supertile
+// stride (st_desc holds the first supertile id and width | height << 16).
+void launch_emit_supertiles(const uint32_t* order, const uint2* st_desc, uint32_t S, const uint32_t* S_dev,
+                            const unsigned long long* block_sums, uint32_t* keys, uint32_t* vals, uint32_t cap, int* overflow,
+                            const uint32_t* total, uint32_t* eff, const DevCam* cams, uint32_t n_per_view, int grid,
+                            cudaStream_t st);
+
+// supertile.cu: the tile lists from the supertile-sorted entries.
+struct SupertileArgs {
+    const DevCam* cams;
+    int nviews;
+    const uint32_t* ent_key;       // sorted entries: supertile id
+    const uint32_t* ent_slot;      // sorted entries: slot
+    const uint32_t* n_ent;         // device count of the sorted entries
+    const uint2* tdesc;            // per slot: first CTA tile, rect width | height << 16
+    const float4* rec;             // splat records (three planes of S)
+    uint32_t S;
+    int tile_w, tile_h, prune;
+    uint16_t* masks;               // per entry: the supertile's tiles it keeps (bit = row * 4 + col)
+    uint32_t* chunk_cnt;           // [tile position][chunk_stride] entries per chunk, scanned in place
+    uint32_t chunk_stride;         // supertile_chunks(cap)
+    uint32_t* plane_tot;           // [tile position] entries with that bit
+    uint32_t* vals_out;            // tile lists: slots
+    uint32_t cap;                  // capacity of vals_out (and of the entries)
+    uint2* ranges;                 // [global CTA tile] list range in vals_out; zeroed by the caller
+    int* overflow;
+};
+// chunk_cnt's row length for up to `entries` entries.
+size_t supertile_chunks(size_t entries);
+// Per entry the 16-tile mask, the per-chunk counts and their scans, then the
+// tile lists and the ranges of every tile that some entry's supertile holds.
+void launch_supertile_lists(const SupertileArgs& a, cudaStream_t st);
 
 // blend.cu
 struct BlendArgs {

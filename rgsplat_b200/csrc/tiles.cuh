@@ -81,11 +81,12 @@ __device__ __forceinline__ void cta_tile_box(int tx, int ty, int tw, int th, int
 // x-extent of E within the band is [xl, xr], where xr is E's rightmost point
 // if its y lies in the band, else the larger root of q(x, y_edge) = T at the
 // band edge nearest to it (E's right boundary is concave in y), and likewise
-// for xl. The span is computed with T enlarged by 2 % and widened by half a
-// pixel, so it contains every tile the per-tile test keeps with a margin far
-// above float rounding; the blend still applies the per-tile test.
+// for xl (the roots are formed with 1/a, within an ulp of the quotient). The
+// span is computed with T enlarged by 2 % and widened by half a pixel, so it
+// contains every tile the per-tile test keeps with a margin far above float
+// rounding; the blend still applies the per-tile test.
 struct SpanSetup {
-    float sx, sy, a, b, c, T, xr, yr;
+    float sx, sy, a, b, c, T, xr, yr, ia;  // ia = 1 / a
     bool testable;
 };
 
@@ -97,6 +98,7 @@ __device__ __forceinline__ SpanSetup span_setup(float sx, float sy, float a, flo
     const float det = a * c - b * b;
     u.xr = u.testable ? sqrtf(u.T * c / det) : 0.0f;
     u.yr = u.testable ? -b / c * u.xr : 0.0f;
+    u.ia = u.testable ? 1.0f / a : 0.0f;
     return u;
 }
 
@@ -118,7 +120,7 @@ __device__ __forceinline__ void kept_cols(const SpanSetup& u, int ty, int tw, in
             c1 = c0;
             return;
         }
-        xr = (-u.b * er + sqrtf(disc)) / u.a;
+        xr = (-u.b * er + sqrtf(disc)) * u.ia;
     }
     const float el = fminf(fmaxf(-u.yr, ly), hy);
     if (el == -u.yr) {
@@ -129,13 +131,15 @@ __device__ __forceinline__ void kept_cols(const SpanSetup& u, int ty, int tw, in
             c1 = c0;
             return;
         }
-        xl = (-u.b * el - sqrtf(disc)) / u.a;
+        xl = (-u.b * el - sqrtf(disc)) * u.ia;
     }
     // pixel-space interval, widened by half a pixel; a tile's pixel centres
     // span [tx * tw + 0.5, tx * tw + tw - 0.5]
     const float X0 = u.sx + xl - 0.5f, X1 = u.sx + xr + 0.5f;
-    const float f0 = floorf((X0 + 0.5f) / (float)tw - 1.0f);
-    const float f1 = floorf((X1 - 0.5f) / (float)tw) + 1.0f;
+    // tile widths are powers of two, so multiplying by 1 / tw is exact
+    const float itw = 1.0f / (float)tw;
+    const float f0 = floorf((X0 + 0.5f) * itw - 1.0f);
+    const float f1 = floorf((X1 - 0.5f) * itw) + 1.0f;
     c0 = (int)fminf(fmaxf(f0, (float)cx0), (float)cx1);
     c1 = (int)fminf(fmaxf(f1, (float)cx0), (float)cx1);
     if (c1 < c0) c1 = c0;
