@@ -190,21 +190,26 @@ def render_targets(R, scenes, cfg, g, ctx):
     return targets
 
 
-def algorithmic_bytes(stage: str, n: int, views: int, pairs: int, pixels: int, visible: int) -> float:
+def algorithmic_bytes(stage: str, n: int, views: int, pairs: int, pixels: int, visible: int, entries: int) -> float:
     """Per-step algorithmic HBM bytes of a stage: what an ideal kernel must
     move, each datum once (S = views * n slots; `visible` = slots with at
-    least one tile pair; a splat record is 48 B, a Gaussian 240 B)."""
+    least one tile pair; `entries` = (supertile, slot) entries; a splat record
+    is 48 B, a Gaussian 240 B)."""
     S = views * n
     if stage == "project":
-        return n * 240.0 + S * (48 + 4 + 8 + 4 + 4)               # params once; record, count, rect, key, id per slot
+        return n * 240.0 + S * (48 + 4 + 8 + 8 + 4 + 4)           # params once; record, count, rect, spans, key, id per slot
     if stage == "depth_sort":
-        return S * 8.0 * 2                                         # (key, slot) read + written once
+        # compaction: count + key per slot read; key, slot, supertile count + rect per visible slot
+        # written; sort: (key, slot) read + written once
+        return S * 8.0 + visible * (8 + 12) + visible * 8.0 * 2
     if stage == "emit":
-        return S * 8.0 + visible * (8 + 32) + pairs * 8.0          # order + counts; rect + record part per visible slot; pairs
-    if stage == "tile_sort":
-        return pairs * 8.0 * 2                                     # (tile, slot) read + written once
-    if stage == "ranges":
-        return pairs * 4.0
+        # two count scans (order + count), then order + supertile rect per visible slot; entries written
+        return visible * (8 + 8) + visible * (4 + 8) + entries * 8.0
+    if stage == "supertile_sort":
+        return entries * 8.0 * 2                                   # (supertile, slot) read + written once
+    if stage == "tile_lists":
+        # entries read; rect + packed spans per visible slot; one slot per pair written
+        return entries * 8.0 + visible * (8 + 8) + pairs * 4.0
     if stage == "forward":
         return pairs * 4.0 + visible * 48.0 + pixels * 20.0        # pair list, records once; rgb, T, last written
     if stage == "loss":
@@ -621,7 +626,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     # render + backward (no Adam) per set after the timed runs, reading the
     # pass's pair / visible-slot counts and the (pixel, splat) pairs the blend
     # kernels evaluated (rgs_trainer_evaluated_pairs)
-    work = {"pairs": [], "visible": [], "eval_fwd": [], "eval_bwd": []}
+    work = {"pairs": [], "visible": [], "entries": [], "eval_fwd": [], "eval_bwd": []}
     with torch.cuda.stream(stream):
         for vs in timed_views:
             trainer.backward(vs, loss_cfg=lcfg, mode=R.Trainer.BATCHED)
@@ -629,10 +634,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             ef, eb = trainer.evaluated_pairs()
             work["pairs"].append(st_w["pairs"])
             work["visible"].append(st_w["visible"])
+            work["entries"].append(st_w["supertile_entries"])
             work["eval_fwd"].append(ef)
             work["eval_bwd"].append(eb)
     pairs_step = float(np.mean(work["pairs"]))
     visible_step = float(np.mean(work["visible"]))
+    entries_step = float(np.mean(work["entries"]))
     eval_fwd, eval_bwd = float(np.mean(work["eval_fwd"])), float(np.mean(work["eval_bwd"]))
 
     # roofline of the dominant stage
@@ -647,7 +654,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     roofline = None
     stages = {}
     for k, ms in per_step_ms.items():
-        b = algorithmic_bytes(k, n, V, pairs_step, pixels_per_step, visible_step)
+        b = algorithmic_bytes(k, n, V, pairs_step, pixels_per_step, visible_step, entries_step)
         gbs = b / (ms / 1e3) / 1e9 if ms > 0 else 0.0
         stages[k] = {"ms": round(ms, 4), "algorithmic_gb": round(b / 1e9, 4), "achieved_gbs": round(gbs, 1), "frac_hbm": round(gbs / hbm, 4)}
     # FP32 roofline of the blend kernels: evaluated (pixel, splat) pairs x the
@@ -668,7 +675,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                    "pairs_per_ns": round(pairs_eval / (ms * 1e6), 3)}
         stages[k]["fp32"] = fp32[k]
     if dom:
-        b = algorithmic_bytes(dom, n, V, pairs_step, pixels_per_step, visible_step)
+        b = algorithmic_bytes(dom, n, V, pairs_step, pixels_per_step, visible_step, entries_step)
         ach = b / (per_step_ms[dom] / 1e3) / 1e9
         traffic = profiled_traffic("blend_bwd_1M_8views.md") if dom == "backward" and args.scale == 1.0 else None
         roofline = {"bound": "hbm", "kernel": dom, "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
@@ -702,7 +709,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             "mode": "batched (graph-captured, one launch per stage)",
             "layout": {"tile": layout[0], "batch": layout[1], "pixels_per_thread": layout[2], "autotune": tune},
             "plain": {"value": round(plain_value, 4), "unit": UNIT, "steps": kp, "batched_over_plain": round(value / plain_value, 3)},
-            "work_per_step": {"pairs": int(pairs_step), "visible_slots": int(visible_step), "pixels": pixels_per_step,
+            "work_per_step": {"pairs": int(pairs_step), "visible_slots": int(visible_step),
+                              "supertile_entries": int(entries_step), "pixels": pixels_per_step,
                               "evaluated_pairs_forward": int(eval_fwd), "evaluated_pairs_backward": int(eval_bwd),
                               "measured_on": "an untimed render + backward of each timed view set after the timed runs"},
             "e2e": e2e,
@@ -716,12 +724,16 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             line["backward_variants"] = measure_backward_variants(R, scenes, local_rank)
         if not args.no_rows and world == 1:
             line["next_rows"] = measure_next_rows(R, g, cfg.cameras[0], local_rank, cpu=not args.no_cpu_baseline)
-        # kernels launched per batched step: term cache + project 2, depth sort 4x3, count
-        # scan 2, emit 1, tile sort 3 per 8 bits, ranges 1, forward 1, loss 2,
-        # backward 1, geometry+Adam 3 (per view, SH half, geometry half) (+ memsets)
+        # kernels launched per batched step (+ memsets): term cache + project 2;
+        # compaction 3 (counts, scan, gather); depth sort 4 passes x 3; two
+        # count scans 2 x 2; emit 1; supertile sort 3 per 8 bits of the
+        # supertile id; tile lists 3 (masks, scan, writer); forward 1; loss 2;
+        # backward 1; geometry + Adam 3 (per view, SH half, geometry half)
         ltw, lth = (int(x) for x in layout[0].split("x"))
-        tile_bits = max(1, int(np.ceil(np.log2(max(2, V * max(-(-c.width // ltw) * -(-c.height // lth) for c in cfg.cameras))))))
-        per_step = 2 + 12 + 2 + 1 + 3 * ((tile_bits + 7) // 8) + 1 + 1 + 2 + 1 + 3
+        cdiv = lambda a, b: -(-a // b)
+        st_view = max(cdiv(cdiv(c.width, ltw), 4) * cdiv(cdiv(c.height, lth), 4) for c in cfg.cameras)
+        st_bits = max(1, int(np.ceil(np.log2(max(2, V * st_view)))))
+        per_step = 2 + 3 + 12 + 4 + 1 + 3 * ((st_bits + 7) // 8) + 3 + 1 + 2 + 1 + 3
         line["gpu_launches"] = per_step * args.steps
         print(json.dumps(line), flush=True)
     if dist is not None:

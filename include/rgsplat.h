@@ -327,13 +327,17 @@ int rgs_trainer_set_adam_state(rgs_ctx* ctx, const rgs_adam_state* state);
  * default stream), or on the context's own stream when NULL. */
 int rgs_set_stream(rgs_ctx* ctx, void* cuda_stream);
 
-/* Per-stage device timing of trainer steps (CUDA events between stages). */
+/* Per-stage device timing of trainer steps (CUDA events between stages):
+ * projection; compaction of the splats with tile pairs + depth sort; count
+ * scans + (supertile, splat) entry emission; supertile sort; per-tile lists
+ * (masks, scans, list writer); forward blend; loss; backward blend; geometry
+ * backward + Adam. */
 #define RGS_NUM_STAGES 9
 #define RGS_STAGE_PROJECT 0
 #define RGS_STAGE_DEPTH_SORT 1
 #define RGS_STAGE_EMIT 2
-#define RGS_STAGE_TILE_SORT 3
-#define RGS_STAGE_RANGES 4
+#define RGS_STAGE_SUPERTILE_SORT 3
+#define RGS_STAGE_TILE_LISTS 4
 #define RGS_STAGE_FORWARD 5
 #define RGS_STAGE_LOSS 6
 #define RGS_STAGE_BACKWARD 7
@@ -352,6 +356,8 @@ typedef struct rgs_stats {
     uint32_t view_groups;   /* groups the last batched step ran as: 1, or more
                                when its pairs passed 2^30 (each group within it) */
     uint32_t reserved;
+    uint64_t supertile_entries; /* (supertile, splat) entries binned: each splat once
+                                   per 4x4-tile supertile its tile rectangle meets */
 } rgs_stats;
 int rgs_get_stats(rgs_ctx* ctx, rgs_stats* out);
 

@@ -29,6 +29,13 @@ int rgs_debug_project(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_
 int rgs_debug_tile_lists(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, uint64_t* n_pairs,
                          int32_t* offsets, int32_t* entries, size_t cap);
 
+/* The same lists pruned as the zero-background render and training paths bin
+ * them: each splat only in the tiles of its rows' kept spans (a conservative
+ * superset of the tiles whose pixels its alpha can reach). *n_pairs is the
+ * pair count the projection made, which the lists must hold exactly. */
+int rgs_debug_pruned_tile_lists(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera,
+                                uint64_t* n_pairs, int32_t* offsets, int32_t* entries, size_t cap);
+
 /* forward_pass caches (backward.rs:296-385): rgb w*h*3, final T w*h, last
  * contributor (index into the pixel's tile list, -1 if none) w*h. */
 int rgs_debug_forward(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, const float bg[3],

@@ -26,7 +26,7 @@ RGS_ERR_FORMAT = -9
 RGS_STEP_PLAIN = 0
 RGS_STEP_BATCHED = 1
 RGS_NUM_STAGES = 9
-STAGE_NAMES = ("project", "depth_sort", "emit", "tile_sort", "ranges", "forward", "loss", "backward", "geometry_adam")
+STAGE_NAMES = ("project", "depth_sort", "emit", "supertile_sort", "tile_lists", "forward", "loss", "backward", "geometry_adam")
 RGS_PROJECT_WGSL = 0
 RGS_PROJECT_CPU_MATH = 1
 RGS_FB_RGBA_F32 = 0
@@ -119,6 +119,7 @@ class rgs_stats(C.Structure):
         ("overflow_retries", C.c_uint32),
         ("view_groups", C.c_uint32),
         ("reserved", C.c_uint32),
+        ("supertile_entries", C.c_uint64),
     ]
 
 
@@ -217,6 +218,8 @@ SIGNATURES = {
     "rgs_debug_project": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), C.POINTER(C.c_int32), FP, C.POINTER(C.c_int32)]),
     "rgs_debug_tile_lists": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), C.POINTER(C.c_uint64), C.POINTER(C.c_int32),
                                        C.POINTER(C.c_int32), C.c_size_t]),
+    "rgs_debug_pruned_tile_lists": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), C.POINTER(C.c_uint64),
+                                              C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_size_t]),
     "rgs_debug_forward": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), FP, FP, FP, C.POINTER(C.c_int32)]),
     "rgs_debug_backward": (C.c_int, [CTX, FP, C.c_size_t, C.POINTER(rgs_camera), FP, FP, C.c_float, FP, FP]),
     "rgs_debug_trainer_batch_pixels": (C.c_int, [CTX, C.c_size_t, FP, FP, FP]),

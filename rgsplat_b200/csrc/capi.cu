@@ -91,7 +91,7 @@ struct rgs_ctx {
     StepHdr* hdr_h = nullptr;  // pinned
     StepOut* out_h = nullptr;  // pinned
     DBuf outd;      // StepOut (device)
-    DBuf rec, cnt, tdesc, dkey, ids, acc, gv;
+    DBuf rec, cnt, tdesc, spans, dkey, ids, acc, gv;
     DBuf ckey, cslot, chunk_counts;  // slots with tile pairs, compacted for the depth sort
     // supertile binning: per slot the supertile count and rectangle, per
     // entry the tile mask, per chunk of entries and tile position the counts,
@@ -384,6 +384,7 @@ int ensure_work(rgs_ctx* ctx, size_t S, size_t px, size_t tiles, size_t lblocks,
     CK(ctx->gv.ensure(std::max<size_t>(S, 1) * 4 * sizeof(float4)));
     CK(ctx->cnt.ensure(std::max<size_t>(S, 1) * 4));
     CK(ctx->tdesc.ensure(std::max<size_t>(S, 1) * 8));
+    CK(ctx->spans.ensure(std::max<size_t>(S, 1) * 16));
     CK(ctx->dkey.ensure(std::max<size_t>(S, 1) * 4));
     CK(ctx->ids.ensure(std::max<size_t>(S, 1) * 4));
     CK(ctx->ckey.ensure(std::max<size_t>(S, 1) * 4));
@@ -457,7 +458,7 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
         cudaMemsetAsync(sc + SC_VISIBLE, 0, 4, st);
         launch_project(s.params.as<float4>(), s.n, s.cap, cams_dev, V, ctx->opt.tile_w, ctx->opt.tile_h,
                        ctx->rec.as<float4>(), ctx->cnt.as<uint32_t>(), ctx->tdesc.as<uint2>(), ctx->dkey.as<uint32_t>(),
-                       ctx->ids.as<uint32_t>(), prune ? 1 : 0, sc + SC_VISIBLE, ctx->gcache.as<float4>(), st);
+                       ctx->ids.as<uint32_t>(), prune ? 1 : 0, sc + SC_VISIBLE, ctx->gcache.as<float4>(), ctx->spans.as<uint4>(), st);
     }
     mark(ctx, 1);
     // only the slots with tile pairs go through the depth sort, gathered in
@@ -493,6 +494,7 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
         int rc = ensure_pairs(ctx, std::max(K, KS));
         if (rc) return rc;
         ctx->stats.pairs += K;
+        ctx->stats.supertile_entries += KS;
         // the depth order may live in the sort scratch: size it for the
         // supertile sort now, while nothing is in flight, so that sort never
         // reallocates it
@@ -534,8 +536,10 @@ int bin_batch(rgs_ctx* ctx, Scene& s, const DevCam* cams_dev, int V, size_t tile
     sa.ent_slot = ent_slot;
     sa.n_ent = sc + SC_STEFF;
     sa.tdesc = ctx->tdesc.as<uint2>();
+    sa.spans = ctx->spans.as<uint4>();
     sa.rec = ctx->rec.as<float4>();
     sa.S = (uint32_t)S;
+    sa.n_per_view = (uint32_t)s.n;
     sa.tile_w = ctx->opt.tile_w;
     sa.tile_h = ctx->opt.tile_h;
     sa.prune = prune ? 1 : 0;
@@ -796,7 +800,7 @@ void rgs_destroy(rgs_ctx* ctx) {
         s->params.release(); s->grads.release(); s->m1.release(); s->m2.release(); s->accum.release(); s->denom.release();
     }
     for (auto& t : ctx->targets) t.release();
-    DBuf* bufs[] = {&ctx->hdr, &ctx->outd, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->gcache, &ctx->dkey, &ctx->ids,
+    DBuf* bufs[] = {&ctx->hdr, &ctx->outd, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->spans, &ctx->gcache, &ctx->dkey, &ctx->ids,
                     &ctx->ckey, &ctx->cslot, &ctx->chunk_counts, &ctx->st_cnt, &ctx->st_desc, &ctx->st_masks,
                     &ctx->st_chunks, &ctx->st_planes, &ctx->st_block_sums, &ctx->acc, &ctx->gv, &ctx->pkeys,
                     &ctx->pvals,
@@ -1562,7 +1566,7 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
         CK(cudaMemsetAsync(sc + SC_VISIBLE, 0, 4, ctx->st));
         launch_project(s.params.as<float4>(), s.n, s.cap, cams_dev, V, ctx->opt.tile_w, ctx->opt.tile_h, ctx->rec.as<float4>(),
                        ctx->cnt.as<uint32_t>(), ctx->tdesc.as<uint2>(), ctx->dkey.as<uint32_t>(), ctx->ids.as<uint32_t>(),
-                       zero_bg(bg) ? 1 : 0, sc + SC_VISIBLE, ctx->gcache.as<float4>(), ctx->st);
+                       zero_bg(bg) ? 1 : 0, sc + SC_VISIBLE, ctx->gcache.as<float4>(), ctx->spans.as<uint4>(), ctx->st);
         launch_view_pairs(ctx->cnt.as<uint32_t>(), (uint32_t)s.n, V, ctx->view_pairs.as<unsigned long long>(), ctx->st);
         CK(cudaGetLastError());
         unsigned long long per[MAX_VIEWS], total = 0;
@@ -1579,7 +1583,7 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
         h->bc[1] = 1.0f - powi_f(tc.beta2, (int)s.t);
         // Everything a captured graph bakes in: sizes, every buffer address, and
         // the loss weight, background and optimiser constants.
-        const DBuf* bufs[] = {&s.params, &s.grads, &s.m1, &s.m2, &s.accum, &s.denom, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->gv, &ctx->gcache, &ctx->dkey,
+        const DBuf* bufs[] = {&s.params, &s.grads, &s.m1, &s.m2, &s.accum, &s.denom, &ctx->rec, &ctx->cnt, &ctx->tdesc, &ctx->spans, &ctx->gv, &ctx->gcache, &ctx->dkey,
                               &ctx->ids, &ctx->ckey, &ctx->cslot, &ctx->chunk_counts, &ctx->st_cnt, &ctx->st_desc,
                               &ctx->st_masks, &ctx->st_chunks, &ctx->st_planes, &ctx->st_block_sums,
                               &ctx->acc, &ctx->pkeys,
@@ -1627,6 +1631,7 @@ int batched_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], 
         }
         if (ctx->out_h->sort_fault) return fail(ctx, RGS_ERR_CUDA, "a sort pass's staged copies timed out");
         ctx->stats.pairs = ctx->out_h->pairs64;
+        ctx->stats.supertile_entries = ctx->out_h->st_pairs64;
         ctx->stats.visible = ctx->out_h->visible;
         ctx->stats.view_groups = 1;
         if (!ctx->out_h->overflow) {
@@ -1664,7 +1669,7 @@ int split_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], fl
     CK(cudaMemcpyAsync(per, ctx->view_pairs.p, sizeof(unsigned long long) * V, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     int groups = 0;
-    unsigned long long total = 0;
+    unsigned long long total = 0, total_st = 0;
     for (int v0 = 0; v0 < V;) {
         int v1 = v0 + 1;
         unsigned long long k = per[v0];
@@ -1677,10 +1682,12 @@ int split_step(rgs_ctx* ctx, const uint32_t* views, int V, const float bg[3], fl
                           host_targets ? host_targets + v0 : nullptr, groups > 0 ? 1 : 0, false);
         if (rc) return rc;
         total += ctx->stats.pairs;
+        total_st += ctx->stats.supertile_entries;
         ++groups;
         v0 = v1;
     }
     ctx->stats.pairs = total;
+    ctx->stats.supertile_entries = total_st;
     ctx->stats.view_groups = (uint32_t)groups;
     ctx->batch_views = 0;
     if (!fused) return RGS_OK;
@@ -2102,7 +2109,7 @@ namespace {
 
 // Uploads gaussians + camera into the scratch scene and bins one view.
 int debug_bin(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, DevCam& dc, DevCam** cams_dev,
-              Binned& b, size_t& px, size_t& tiles, size_t& lb) {
+              Binned& b, size_t& px, size_t& tiles, size_t& lb, bool prune = false) {
     if (!camera || (n && !gaussians)) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
     int rc = make_devcam(ctx, *camera, dc);
     if (rc) return rc;
@@ -2113,7 +2120,7 @@ int debug_bin(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* 
     if ((rc = ensure_work(ctx, std::max<size_t>(n, 1), px, tiles, lb, 1))) return rc;
     if ((rc = upload_single_cam(ctx, dc, cams_dev))) return rc;
     if ((rc = ensure_gcache(ctx, s))) return rc;
-    return bin_batch(ctx, s, *cams_dev, 1, tiles, true, b);
+    return bin_batch(ctx, s, *cams_dev, 1, tiles, true, b, true, prune);
 }
 
 }  // namespace
@@ -2157,15 +2164,16 @@ int rgs_debug_project(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_
     return RGS_OK;
 }
 
-int rgs_debug_tile_lists(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, uint64_t* n_pairs,
-                         int32_t* offsets, int32_t* entries, size_t cap) {
+namespace {
+int debug_tile_lists(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, uint64_t* n_pairs,
+                     int32_t* offsets, int32_t* entries, size_t cap, bool prune) {
     int rc = check_ctx(ctx);
     if (rc) return rc;
     if (!n_pairs) return fail(ctx, RGS_ERR_INVALID_ARG, "null argument");
     DevCam dc, *cams_dev;
     Binned b;
     size_t px, tiles, lb;
-    if ((rc = debug_bin(ctx, gaussians, n, camera, dc, &cams_dev, b, px, tiles, lb))) return rc;
+    if ((rc = debug_bin(ctx, gaussians, n, camera, dc, &cams_dev, b, px, tiles, lb, prune))) return rc;
     uint32_t K = 0;
     CK(cudaMemcpyAsync(&K, ctx->scalars.as<uint32_t>() + SC_PAIRS, 4, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
@@ -2189,6 +2197,17 @@ int rgs_debug_tile_lists(rgs_ctx* ctx, const float* gaussians, size_t n, const r
     offsets[tiles] = (int32_t)k;
     if (k != K) return fail(ctx, RGS_ERR_CUDA, "internal: tile lists do not hold every pair");
     return RGS_OK;
+}
+}  // namespace
+
+int rgs_debug_tile_lists(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, uint64_t* n_pairs,
+                         int32_t* offsets, int32_t* entries, size_t cap) {
+    return debug_tile_lists(ctx, gaussians, n, camera, n_pairs, offsets, entries, cap, false);
+}
+
+int rgs_debug_pruned_tile_lists(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera,
+                                uint64_t* n_pairs, int32_t* offsets, int32_t* entries, size_t cap) {
+    return debug_tile_lists(ctx, gaussians, n, camera, n_pairs, offsets, entries, cap, true);
 }
 
 int rgs_debug_forward(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs_camera* camera, const float bg[3], float* rgb,

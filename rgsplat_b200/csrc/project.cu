@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(256, 5) k_project(const float4* __restrict__ p
                                                  int tile_h, float4* __restrict__ rec, uint32_t* __restrict__ cnt,
                                                  uint2* __restrict__ tdesc, uint32_t* __restrict__ dkey,
                                                  uint32_t* __restrict__ ids, int prune, uint32_t* __restrict__ visible,
-                                                 const float4* __restrict__ gcache) {
+                                                 const float4* __restrict__ gcache, uint4* __restrict__ spans) {
     // chunk-major grid: the nviews consecutive blocks project the same 256
     // Gaussians into every view, so the per-Gaussian reads (SH, position,
     // cached terms) of all but the first view come from L2
@@ -187,14 +187,26 @@ __global__ void __launch_bounds__(256, 5) k_project(const float4* __restrict__ p
     rec[2 * S + s] = make_float4(o.color[0], o.color[1], o.color[2], __uint_as_float((uint32_t)y0 | ((uint32_t)y1 << 16)));
     uint32_t count = (uint32_t)((ctx1 - ctx0) * (cty1 - cty0));
     if (prune) {
-        // only the tiles of each row's kept span (tiles.cuh)
+        // only the tiles of each row's kept span (tiles.cuh); rectangles of
+        // at most SPAN_ROWS rows and 15 columns keep their spans packed for
+        // the tile lists (byte r: first kept column - ctx0 | count << 4)
         const SpanSetup u = span_setup(o.sx, o.sy, o.conic[0], o.conic[1], o.conic[2], power_floor(o.opacity));
+        const bool pack = ctx1 - ctx0 <= 15 && cty1 - cty0 <= SPAN_ROWS;
+        unsigned long long lo = 0, hi = 0;
         count = 0;
         for (int ty = cty0; ty < cty1; ++ty) {
             int c0, c1;
             kept_cols(u, ty, tile_w, tile_h, c.height, ctx0, ctx1, c0, c1);
             count += (uint32_t)(c1 - c0);
+            const unsigned long long b = (uint32_t)(c0 - ctx0) | ((uint32_t)(c1 - c0) << 4);
+            const int r = ty - cty0;
+            if (pack) {
+                if (r < 8) lo |= b << (8 * r);
+                else hi |= b << (8 * (r - 8));
+            }
         }
+        spans[s] = pack ? make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32))
+                        : make_uint4(SPANS_NONE, SPANS_NONE, SPANS_NONE, SPANS_NONE);
     }
     cnt[s] = count;
     if (count) {
@@ -209,13 +221,13 @@ __global__ void __launch_bounds__(256, 5) k_project(const float4* __restrict__ p
 
 void launch_project(const float4* params, int n, int cap, const DevCam* cams, int nviews, int tile_w, int tile_h,
                     float4* rec, uint32_t* cnt, uint2* tdesc, uint32_t* dkey, uint32_t* ids, int prune, uint32_t* visible,
-                    float4* gcache, cudaStream_t st) {
+                    float4* gcache, uint4* spans, cudaStream_t st) {
     size_t S = (size_t)n * nviews;
     if (S == 0) return;
     launch_gauss_cache(params, n, cap, gcache, st);
     unsigned blocks = (unsigned)(((size_t)n + 255) / 256 * (size_t)nviews);
     k_project<<<blocks, 256, 0, st>>>(params, n, cap, cams, nviews, tile_w, tile_h, rec, cnt, tdesc, dkey, ids, prune, visible,
-                                      gcache);
+                                      gcache, spans);
 }
 
 // ---------------------------------------------------------------------------

@@ -165,9 +165,16 @@ void launch_check_finite(const float4* planes, int n, int cap, int* flag, cudaSt
 // its CTA-tile rectangle), cnt[s] = its number of CTA tiles, or with prune = 1
 // the number inside the rows' kept spans (tiles.cuh); zero for culled slots.
 // *visible (zeroed by the caller) gains the number of slots with cnt > 0.
+// With prune, spans[slot] holds the kept spans of rectangles up to SPAN_ROWS
+// rows and 15 columns, byte r of the 16 (x holds rows 0-3, y 4-7, ...): first
+// kept column - first rectangle column | kept count << 4. Larger rectangles
+// get SPANS_NONE in every word (a byte 0xff never occurs in a packed record:
+// the first column and the count add up to at most 15).
+constexpr int SPAN_ROWS = 16;
+constexpr uint32_t SPANS_NONE = 0xffffffffu;
 void launch_project(const float4* params, int n, int cap, const DevCam* cams, int nviews,
                     int tile_w, int tile_h, float4* rec, uint32_t* cnt, uint2* tdesc, uint32_t* dkey,
-                    uint32_t* ids, int prune, uint32_t* visible, float4* gcache, cudaStream_t st);
+                    uint32_t* ids, int prune, uint32_t* visible, float4* gcache, uint4* spans, cudaStream_t st);
 // Per-Gaussian view-independent projection terms ([2][cap] float4: opacity
 // and the 3D covariance's six entries), computed by launch_project first and
 // read by the geometry of the same step.
@@ -221,8 +228,10 @@ struct SupertileArgs {
     const uint32_t* ent_slot;      // sorted entries: slot
     const uint32_t* n_ent;         // device count of the sorted entries
     const uint2* tdesc;            // per slot: first CTA tile, rect width | height << 16
+    const uint4* spans;            // per slot (with prune): packed kept spans, or SPANS_NONE
     const float4* rec;             // splat records (three planes of S)
     uint32_t S;
+    uint32_t n_per_view;           // slot = view * n_per_view + Gaussian
     int tile_w, tile_h, prune;
     uint16_t* masks;               // per entry: the supertile's tiles it keeps (bit = row * 4 + col)
     uint32_t* chunk_cnt;           // [tile position][chunk_stride] entries per chunk, scanned in place

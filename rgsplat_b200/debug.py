@@ -27,9 +27,11 @@ def project(gaussians, camera: Camera, ctx: Context | None = None):
     return vis[:n], rec[:n], rect[:n]
 
 
-def tile_lists(gaussians, camera: Camera, ctx: Context | None = None):
-    """-> (offsets (tiles+1,), entries (pairs,)) over the context's CTA tiles."""
+def tile_lists(gaussians, camera: Camera, ctx: Context | None = None, pruned: bool = False):
+    """-> (offsets (tiles+1,), entries (pairs,)) over the context's CTA tiles;
+    pruned: the lists the zero-background paths bin (rgs_debug_pruned_tile_lists)."""
     ctx = ctx or default_context()
+    fn = ctx.lib.rgs_debug_pruned_tile_lists if pruned else ctx.lib.rgs_debug_tile_lists
     g = _gauss(gaussians)
     n = g.shape[0]
     cam = camera_c(camera)
@@ -38,11 +40,11 @@ def tile_lists(gaussians, camera: Camera, ctx: Context | None = None):
     tiles = ((camera.width + tw - 1) // tw) * ((camera.height + th - 1) // th)
     npairs = C.c_uint64(0)
     ip = C.POINTER(C.c_int32)
-    ctx.check(ctx.lib.rgs_debug_tile_lists(ctx.handle, _fp(g), n, C.byref(cam), C.byref(npairs), None, None, 0))
+    ctx.check(fn(ctx.handle, _fp(g), n, C.byref(cam), C.byref(npairs), None, None, 0))
     offs = np.zeros(tiles + 1, np.int32)
     ent = np.zeros(max(int(npairs.value), 1), np.int32)
-    ctx.check(ctx.lib.rgs_debug_tile_lists(ctx.handle, _fp(g), n, C.byref(cam), C.byref(npairs), offs.ctypes.data_as(ip),
-                                           ent.ctypes.data_as(ip), ent.shape[0]))
+    ctx.check(fn(ctx.handle, _fp(g), n, C.byref(cam), C.byref(npairs), offs.ctypes.data_as(ip), ent.ctypes.data_as(ip),
+                 ent.shape[0]))
     return offs, ent[: int(npairs.value)]
 
 

@@ -107,6 +107,33 @@ def test_pruned_tile_lists_render_identically(ctx):
     assert 0 < pruned < ent.size
 
 
+def test_pruned_lists_are_ordered_subsets_of_the_full_lists(ctx):
+    """Pruned lists (zero background): each tile's list is the reference's
+    full list with splats left out and the order kept, and together they hold
+    exactly the pair count the projection made (rgs_debug_pruned_tile_lists
+    fails otherwise). The scene mixes small splats, whose kept spans the
+    projection packs, with splats whose tile rectangles pass 8 rows or 15
+    columns, whose spans the list builder recomputes per supertile."""
+    g, cam, _ = small_scene(n=3000, seed=12, w=640, h=480)
+    g = g.copy()
+    rng = np.random.default_rng(12)
+    big = rng.choice(g.shape[0], 150, replace=False)
+    g[big, 7:10] += np.float32(np.log(12.0))
+    vis, _, rect = D.project(g, cam, ctx)
+    wide = (vis != 0) & (((rect[:, 3] - rect[:, 1]) > 8) | ((rect[:, 2] - rect[:, 0]) > 15))
+    assert wide.sum() >= 5
+    offs_f, ent_f = D.tile_lists(g, cam, ctx)
+    offs_p, ent_p = D.tile_lists(g, cam, ctx, pruned=True)
+    assert offs_p.shape == offs_f.shape
+    assert 0 < ent_p.size < ent_f.size
+    for t in range(offs_f.size - 1):
+        full = iter(ent_f[offs_f[t]:offs_f[t + 1]].tolist())
+        assert all(x in full for x in ent_p[offs_p[t]:offs_p[t + 1]].tolist()), f"tile {t}"
+    rgb = R.render_color(g, cam, (0.0, 0.0, 0.0), ctx=ctx)
+    orgb, _, _ = O.render_color(g, cam, (0.0, 0.0, 0.0))
+    assert np.array_equal(rgb.reshape(-1).view(np.uint32), orgb.reshape(-1).view(np.uint32))
+
+
 def test_render_color_odd_sizes(ctx):
     g, cam, _ = small_scene(n=3000, seed=6, w=173, h=91, fx=200.0)
     rgb = R.render_color(g, cam, (0.1, 0.1, 0.1), ctx=ctx)
