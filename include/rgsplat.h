@@ -108,6 +108,10 @@ typedef struct rgs_options {
                                   runs as consecutive view groups within it (gradients summed
                                   across groups, one Adam step); 0 = default 2^30 (pair buffers
                                   and sort scratch take 16 bytes per pair) */
+    int exact_loss;       /* 0 (default): the SSIM blurs accumulate with fused multiply-adds
+                             (dL/dpixel within float rounding of the reference's); 1: the
+                             reference's separate multiply and add and its divisions
+                             (backward.rs:718-807), dL/dpixel bit-identical */
 } rgs_options;
 
 /* Step modes of rgs_trainer_step. */

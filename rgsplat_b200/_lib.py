@@ -107,6 +107,7 @@ class rgs_options(C.Structure):
         ("reference_compat", C.c_int),
         ("pixels_per_thread", C.c_int),
         ("batch_pair_limit", C.c_uint64),
+        ("exact_loss", C.c_int),
     ]
 
 

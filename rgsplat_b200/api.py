@@ -140,10 +140,14 @@ class AdamState:
 # context
 # ---------------------------------------------------------------------------
 class Context:
-    """One CUDA stream plus the library's device buffers (``rgs_ctx``)."""
+    """One CUDA stream plus the library's device buffers (``rgs_ctx``).
+
+    exact_loss: the SSIM blurs use the reference's separate multiply and add
+    (dL/dpixel bit-identical to the reference's) instead of fused
+    multiply-adds (the default; within float rounding)."""
 
     def __init__(self, device: int = 0, tile: tuple[int, int] = (16, 16), batch: int = 256, reference_compat: bool = True,
-                 pixels_per_thread: int = 2, batch_pair_limit: int = 0):
+                 pixels_per_thread: int = 2, batch_pair_limit: int = 0, exact_loss: bool = False):
         self.lib = L.load()
         o = L.rgs_options()
         self.lib.rgs_options_default(C.byref(o))
@@ -153,6 +157,7 @@ class Context:
         o.reference_compat = 1 if reference_compat else 0
         o.pixels_per_thread = int(pixels_per_thread)
         o.batch_pair_limit = int(batch_pair_limit)
+        o.exact_loss = 1 if exact_loss else 0
         h = C.c_void_p()
         rc = self.lib.rgs_create(C.byref(o), C.byref(h))
         if rc != L.RGS_OK:

@@ -659,7 +659,7 @@ int run_view_plain(rgs_ctx* ctx, Scene& s, const DevCam& dc_in, const float* tar
     if (!do_backward) return RGS_OK;
     float* losses_dev = (float*)((char*)ctx->outd.p + offsetof(StepOut, losses));
     CK(launch_loss(cams_dev, 1, (int)lb, ctx->rgb.as<float>(), lambda, ctx->dl.as<float>(), ctx->partials.as<float>(),
-                   losses_dev, nullptr, st));
+                   losses_dev, nullptr, ctx->opt.exact_loss != 0, st));
     mark(ctx, 7);
     CK(cudaMemsetAsync(ctx->acc.p, 0, std::max<size_t>(s.n, 1) * 3 * sizeof(float4), st));
     BlendArgs ba = blend_args(ctx, s, cams_dev, 1, nullptr, tiles, b, bg, false);
@@ -713,6 +713,7 @@ void rgs_options_default(rgs_options* o) {
     o->reference_compat = 1;
     o->pixels_per_thread = 2;
     o->batch_pair_limit = 0;
+    o->exact_loss = 0;
 }
 
 void rgs_train_config_default(rgs_train_config* c) {
@@ -1026,7 +1027,7 @@ int rgs_photometric_loss_grad(rgs_ctx* ctx, const float* rendered_rgb, const flo
     if ((rc = upload_single_cam(ctx, dc, &cams_dev))) return rc;
     float* losses_dev = (float*)((char*)ctx->outd.p + offsetof(StepOut, losses));
     CK(launch_loss(cams_dev, 1, (int)lb, ctx->rgb.as<float>(), lambda, ctx->dl.as<float>(), ctx->partials.as<float>(),
-                   losses_dev, nullptr, ctx->st));
+                   losses_dev, nullptr, ctx->opt.exact_loss != 0, ctx->st));
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(loss_out, losses_dev, 4, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemcpyAsync(dl_out, ctx->dl.p, px * 12, cudaMemcpyDeviceToHost, ctx->st));
@@ -1474,7 +1475,8 @@ int capture_batched(rgs_ctx* ctx, int V, size_t tiles_cap, const float bg[3], fl
         // just before this graph's launch; only the loss waits for them
         if (host_targets) cudaStreamWaitEvent(st, ctx->ev_copy, cudaEventWaitExternal);
         cudaError_t le = launch_loss(cams_dev, V, 0, ctx->rgb.as<float>(), lambda, ctx->dl.as<float>(),
-                                     ctx->partials.as<float>(), losses_dev, &hd->total_loss_blocks, st);
+                                     ctx->partials.as<float>(), losses_dev, &hd->total_loss_blocks,
+                                     ctx->opt.exact_loss != 0, st);
         if (le != cudaSuccess) rc = cuda_fail(ctx, le, "loss kernel launch");
         mark(ctx, 7);
         cudaMemsetAsync(ctx->acc.p, 0, std::max<size_t>(S, 1) * 3 * sizeof(float4), st);
@@ -2246,7 +2248,7 @@ int rgs_debug_backward(rgs_ctx* ctx, const float* gaussians, size_t n, const rgs
     launch_blend_forward(fa, ctx->opt.tile_w, ctx->opt.tile_h, ctx->opt.batch, ctx->st);
     float* losses_dev = (float*)((char*)ctx->outd.p + offsetof(StepOut, losses));
     CK(launch_loss(cams_dev, 1, (int)lb, ctx->rgb.as<float>(), lambda, ctx->dl.as<float>(), ctx->partials.as<float>(),
-                   losses_dev, nullptr, ctx->st));
+                   losses_dev, nullptr, ctx->opt.exact_loss != 0, ctx->st));
     CK(cudaMemsetAsync(ctx->acc.p, 0, std::max<size_t>(n, 1) * 3 * sizeof(float4), ctx->st));
     BlendArgs ba = blend_args(ctx, ctx->sc, cams_dev, 1, nullptr, tiles, b, bg, false);
     launch_blend_backward(ba, ctx->opt.tile_w, ctx->opt.tile_h, ctx->opt.batch, ctx->st);

@@ -11,8 +11,8 @@
 // address is looked up with cudaGetSymbolAddress, with the device current,
 // on the first call on each device (that first call also sets the loss
 // kernel's shared-memory limit; it should come before any stream capture).
-// The kernels are the ones rgs_photometric_loss_grad runs (loss.cu); only
-// where their scratch lives differs.
+// The kernels are the ones rgs_photometric_loss_grad runs (loss.cu) with the
+// default options (fused blur taps); only where their scratch lives differs.
 //
 // The array keeps whatever the previous call left in it, and nothing in it has
 // to start at zero: the header is written by a one-thread kernel on the
@@ -121,7 +121,7 @@ extern "C" int rgs_photometric_loss_grad_noalloc(int device, const float* render
         cudaStream_t st = (cudaStream_t)cuda_stream;
         k_noalloc_put_cam<<<1, 1, 0, st>>>(c, cam_dev);
         if ((e = cudaGetLastError()) == cudaSuccess)
-            e = launch_loss(cam_dev, 1, (int)blocks, rendered_rgb, lambda, dl_out, partials, loss_out, nullptr, st);
+            e = launch_loss(cam_dev, 1, (int)blocks, rendered_rgb, lambda, dl_out, partials, loss_out, nullptr, false, st);
         if (e != cudaSuccess) rc = cuda_err(err, err_len, e);
     }
     cudaSetDevice(prev);

@@ -323,10 +323,11 @@ void launch_unpack_ply(const uint8_t* body, size_t stride, int n, const PlyField
 // limit is a per-device function attribute, set on the current device the
 // first time this is called there (under a mutex; later calls return at once).
 cudaError_t prepare_loss_kernel();
-// Prepares the current device (above), then enqueues the loss kernels.
+// Prepares the current device (above), then enqueues the loss kernels; exact:
+// the reference's separate multiply and add in the blurs (else fused).
 cudaError_t launch_loss(const DevCam* cams, int nviews, int total_blocks, const float* rgb, float lambda,
                         float* dl, float* partials, float* losses, const uint32_t* total_dev,
-                        cudaStream_t st);
+                        bool exact, cudaStream_t st);
 
 // geom.cu
 struct AdamArgs {

@@ -51,7 +51,7 @@ def test_defaults_without_gpu(lib):
     L = _lib.load()
     o = _lib.rgs_options()
     L.rgs_options_default(ctypes.byref(o))
-    assert (o.tile_w, o.tile_h, o.batch, o.reference_compat) == (16, 16, 256, 1)
+    assert (o.tile_w, o.tile_h, o.batch, o.reference_compat, o.exact_loss) == (16, 16, 256, 1, 0)
     c = _lib.rgs_train_config()
     L.rgs_train_config_default(ctypes.byref(c))
     assert abs(c.lr_position - 0.00016) < 1e-9 and c.max_gaussians == 3_000_000

@@ -142,6 +142,17 @@ def test_render_color_odd_sizes(ctx):
 
 
 # ---- loss ------------------------------------------------------------------------
+def assert_dl_close(dl, ref_dl, exact_dl):
+    """dL/dpixel from the fused loss kernel against the reference's f32 values
+    (ref_dl) and the same gradient evaluated in f64 (exact_dl): within 1e-4 of
+    the largest reference entry, and at most twice the reference's own
+    distance from the f64 values."""
+    dl, ref_dl, exact_dl = (np.asarray(a, np.float64).reshape(-1) for a in (dl, ref_dl, exact_dl))
+    scale = np.abs(ref_dl).max()
+    assert np.abs(dl - ref_dl).max() <= 1e-4 * scale
+    assert np.abs(dl - exact_dl).max() <= 2.0 * np.abs(ref_dl - exact_dl).max() + 1e-7 * scale
+
+
 def test_photometric_loss_grad_matches_oracle(ctx):
     rng = np.random.default_rng(7)
     w, h = 77, 53
@@ -149,9 +160,16 @@ def test_photometric_loss_grad_matches_oracle(ctx):
     target = np.concatenate([rng.uniform(0, 1, (h, w, 3)), np.ones((h, w, 1))], axis=2).astype(np.float32)
     loss, dl = R.photometric_loss_grad(rendered, target, w, h, 0.2, ctx=ctx)
     oloss, odl = O.photometric_loss_grad(rendered, target, w, h, 0.2)
+    _, xdl = O.photometric_loss_grad(rendered, target, w, h, 0.2, double=True)
     assert abs(loss - oloss) <= 1e-4 * abs(oloss)
-    # same taps in the same order, separate multiply and add: bit-identical
-    assert np.array_equal(dl.reshape(-1).view(np.uint32), odl.reshape(-1).view(np.uint32))
+    # default: fused multiply-add blur taps, within float rounding of the
+    # reference's dL/dpixel and no further from the f64 evaluation than it
+    assert_dl_close(dl, odl, xdl)
+    # exact_loss: same taps in the same order, separate multiply and add: bit-identical
+    ex = R.Context(exact_loss=True)
+    loss_e, dl_e = R.photometric_loss_grad(rendered, target, w, h, 0.2, ctx=ex)
+    assert abs(loss_e - oloss) <= 1e-4 * abs(oloss)
+    assert np.array_equal(dl_e.reshape(-1).view(np.uint32), odl.reshape(-1).view(np.uint32))
 
 
 def test_image_loss_gradient_matches_finite_difference_gpu(ctx):
