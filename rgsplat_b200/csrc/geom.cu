@@ -224,9 +224,9 @@ __device__ __forceinline__ float adam_lane(float p, float g, float& m1, float& m
 }
 
 // Adam on plane p of Gaussian i (lanes 0..3; plane 2 has only three).
-__device__ __forceinline__ float4 adam_plane(int p, int i, int cap, float4 pv, float4 g, const AdamArgs& a, float bc1, float bc2) {
-    const size_t om = (size_t)p * a.mstride + i;
-    float4 m1 = a.m1[om], m2 = a.m2[om];
+// One plane's update with its moments already loaded (m1, m2 updated in place).
+__device__ __forceinline__ float4 adam_update(int p, float4 pv, float4 g, float4& m1, float4& m2, const AdamArgs& a, float bc1,
+                                              float bc2) {
     const float* lr = a.lr + p * 4;
     pv.x = adam_lane(pv.x, g.x, m1.x, m2.x, lr[0], a, bc1, bc2);
     pv.y = adam_lane(pv.y, g.y, m1.y, m2.y, lr[1], a, bc1, bc2);
@@ -237,6 +237,13 @@ __device__ __forceinline__ float4 adam_plane(int p, int i, int cap, float4 pv, f
         float nrm = sqrtf(pv.x * pv.x + pv.y * pv.y + pv.z * pv.z + pv.w * pv.w);
         if (nrm > 1e-8f) { pv.x /= nrm; pv.y /= nrm; pv.z /= nrm; pv.w /= nrm; }
     }
+    return pv;
+}
+
+__device__ __forceinline__ float4 adam_plane(int p, int i, int cap, float4 pv, float4 g, const AdamArgs& a, float bc1, float bc2) {
+    const size_t om = (size_t)p * a.mstride + i;
+    float4 m1 = a.m1[om], m2 = a.m2[om];
+    pv = adam_update(p, pv, g, m1, m2, a, bc1, bc2);
     a.m1[om] = m1;
     a.m2[om] = m2;
     (void)cap;
@@ -389,6 +396,14 @@ __global__ void __launch_bounds__(128, PART == 2 ? 8 : 6) k_geom_gauss(const flo
 // channel's four SH planes. Sixteen sums per thread instead of forty-eight,
 // so more warps stay resident in this latency-bound pass. Runs before the
 // geometry half, which rewrites the position it reads.
+// The SH half of the per-Gaussian step: block row ch handles colour channel
+// ch's 16 coefficients (planes 3 + 4 ch .. 6 + 4 ch). The per-view slot
+// counts and clamp masks are loaded VIEW_GROUP views at a time before any is
+// used, so the thread waits on two round trips to memory per group instead
+// of two per view; the sums run in view order as before. (Loading all four
+// planes' parameters and moments before the first store as well needed 104
+// registers and ran slower at the lower occupancy.)
+constexpr int VIEW_GROUP = 8;
 __global__ void __launch_bounds__(128, 8) k_geom_sh(int n, int cap, const DevCam* __restrict__ cams, int nviews,
                                                    const uint32_t* __restrict__ cnt, const float4* __restrict__ gv, AdamArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -405,16 +420,22 @@ __global__ void __launch_bounds__(128, 8) k_geom_sh(int n, int cap, const DevCam
     float shg[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) shg[k] = 0.0f;
-    for (int v = 0; v < nviews; ++v) {
-        const size_t s = (size_t)v * n + i;
-        if (cnt[s] == 0) continue;
-        const float mk = mplane[s * 4 + mlane];
-        if (mk == 0.0f) continue;
-        float d[3], basis[16];
-        view_dir(pos, cams[v].pos, d);
-        sh_basis(d, basis);
+    for (int v0 = 0; v0 < nviews; v0 += VIEW_GROUP) {
+        uint32_t c8[VIEW_GROUP];
+        float m8[VIEW_GROUP];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) shg[k] += mk * basis[k];
+        for (int k = 0; k < VIEW_GROUP; ++k) c8[k] = v0 + k < nviews ? cnt[(size_t)(v0 + k) * n + i] : 0u;
+#pragma unroll
+        for (int k = 0; k < VIEW_GROUP; ++k) m8[k] = c8[k] ? mplane[((size_t)(v0 + k) * n + i) * 4 + mlane] : 0.0f;
+#pragma unroll
+        for (int k = 0; k < VIEW_GROUP; ++k) {
+            if (m8[k] == 0.0f) continue;
+            float d[3], basis[16];
+            view_dir(pos, cams[v0 + k].pos, d);
+            sh_basis(d, basis);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) shg[q] += m8[k] * basis[q];
+        }
     }
 #pragma unroll
     for (int kq = 0; kq < 4; ++kq) {
