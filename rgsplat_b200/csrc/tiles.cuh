@@ -52,19 +52,6 @@ __device__ __forceinline__ bool tile_rejects(const TileTest& t, float x0c, float
     return best * 0.999f > -2.0f * t.thr;
 }
 
-// Pixel y range [y0, y1] that can hold a pixel centre where the tile test
-// keeps the splat: the y-extent of E = {q <= -2 thr / 0.999} (sqrt(T a / det)
-// about sy), enlarged by 2 % and half a pixel. False (no bound) for the
-// conics the tile test does not test.
-__device__ __forceinline__ bool splat_y_extent(const TileTest& t, float& y0, float& y1) {
-    if (!t.testable) return false;
-    const float T = -2.0f * t.thr / 0.999f * 1.02f;
-    const float ext = sqrtf(T * t.a / (t.a * t.c - t.b * t.b));
-    y0 = t.sy - ext - 0.5f;
-    y1 = t.sy + ext + 0.5f;
-    return true;
-}
-
 // Pixel-centre box of CTA tile (tx, ty), clipped to the image.
 __device__ __forceinline__ void cta_tile_box(int tx, int ty, int tw, int th, int width, int height, float& x0c, float& x1c,
                                              float& y0c, float& y1c) {
