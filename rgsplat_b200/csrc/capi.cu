@@ -384,7 +384,7 @@ int ensure_work(rgs_ctx* ctx, size_t S, size_t px, size_t tiles, size_t lblocks,
     CK(ctx->gv.ensure(std::max<size_t>(S, 1) * 4 * sizeof(float4)));
     CK(ctx->cnt.ensure(std::max<size_t>(S, 1) * 4));
     CK(ctx->tdesc.ensure(std::max<size_t>(S, 1) * 8));
-    CK(ctx->spans.ensure(std::max<size_t>(S, 1) * 16));
+    CK(ctx->spans.ensure(std::max<size_t>(S, 1) * 32));
     CK(ctx->dkey.ensure(std::max<size_t>(S, 1) * 4));
     CK(ctx->ids.ensure(std::max<size_t>(S, 1) * 4));
     CK(ctx->ckey.ensure(std::max<size_t>(S, 1) * 4));

@@ -101,7 +101,10 @@ __global__ void __launch_bounds__(128, 8) k_geom_view(const float4* __restrict__
     const float tzc = fmaxf(tz, 0.001f);
     float a2d, b2d, c2d;
     {
-        M3 j = {{{fx / tzc, 0.0f, -fx * tx / (tzc * tzc)}, {0.0f, fy / tzc, -fy * ty / (tzc * tzc)}, {0.0f, 0.0f, 0.0f}}};
+        // one reciprocal per denominator (gradients are held to 1e-3 relative,
+        // so the quotients need not round as the reference's divisions)
+        const float itc = 1.0f / tzc, itc2 = itc * itc;
+        M3 j = {{{fx * itc, 0.0f, -fx * tx * itc2}, {0.0f, fy * itc, -fy * ty * itc2}, {0.0f, 0.0f, 0.0f}}};
         M3 t = mul(j, V);
         M3 s2 = mul(mul(t, sig), tr(t));
         a2d = s2.m[0][0] + 0.3f;
@@ -111,12 +114,13 @@ __global__ void __launch_bounds__(128, 8) k_geom_view(const float4* __restrict__
     // conic -> 2D covariance (backward.rs:546-554)
     const float ga = a1.x, gb = a1.y, gc = a1.z;
     const float det = a2d * c2d - b2d * b2d;
-    const float det2 = det * det;
-    const float dl_da = (-ga * c2d * c2d + gb * b2d * c2d - gc * b2d * b2d) / det2;
-    const float dl_db = (2.0f * ga * b2d * c2d - gb * (det + 2.0f * b2d * b2d) + 2.0f * gc * a2d * b2d) / det2;
-    const float dl_dc = (-ga * b2d * b2d + gb * a2d * b2d - gc * a2d * a2d) / det2;
+    const float idet2 = 1.0f / (det * det);
+    const float dl_da = (-ga * c2d * c2d + gb * b2d * c2d - gc * b2d * b2d) * idet2;
+    const float dl_db = (2.0f * ga * b2d * c2d - gb * (det + 2.0f * b2d * b2d) + 2.0f * gc * a2d * b2d) * idet2;
+    const float dl_dc = (-ga * b2d * b2d + gb * a2d * b2d - gc * a2d * a2d) * idet2;
     // T = J W, rows u0, u1 (row 2 of J is zero) (backward.rs:556-564)
-    const float j00 = fx / tz, j02 = -fx * tx / (tz * tz), j11 = fy / tz, j12 = -fy * ty / (tz * tz);
+    const float itz = 1.0f / tz, itz2 = itz * itz, itz3 = itz2 * itz;
+    const float j00 = fx * itz, j02 = -fx * tx * itz2, j11 = fy * itz, j12 = -fy * ty * itz2;
     float u0[3], u1[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -140,7 +144,7 @@ __global__ void __launch_bounds__(128, 8) k_geom_view(const float4* __restrict__
     dS[5] = u0[2] * r0[2] + u1[2] * r1[2];
     // mean through (sx, sy) and through J(pcam) (backward.rs:578-605)
     const float asx = a1.w, asy = a2.x;
-    float dp[3] = {asx * fx / tz, asy * fy / tz, asx * (-fx * tx / (tz * tz)) + asy * (-fy * ty / (tz * tz))};
+    float dp[3] = {asx * j00, asy * j11, asx * j02 + asy * j12};
     {
         // Sigma u0, Sigma u1, Sigma w2 with w2 = row 2 of W
         float su0[3], su1[3], sw2[3];
@@ -150,22 +154,21 @@ __global__ void __launch_bounds__(128, 8) k_geom_view(const float4* __restrict__
             su1[r] = sig.m[r][0] * u1[0] + sig.m[r][1] * u1[1] + sig.m[r][2] * u1[2];
             sw2[r] = sig.m[r][0] * V.m[2][0] + sig.m[r][1] * V.m[2][1] + sig.m[r][2] * V.m[2][2];
         }
-        const float tz2 = tz * tz, tz3 = tz2 * tz;
         // d/dtx: dT row 0 = -fx/tz^2 w2
-        const float ax = -fx / tz2;
+        const float ax = -fx * itz2;
         const float w2su0 = V.m[2][0] * su0[0] + V.m[2][1] * su0[1] + V.m[2][2] * su0[2];
         const float w2su1 = V.m[2][0] * su1[0] + V.m[2][1] * su1[1] + V.m[2][2] * su1[2];
         dp[0] += dl_da * (2.0f * ax * w2su0) + dl_db * (ax * w2su1);
         // d/dty: dT row 1 = -fy/tz^2 w2
-        const float ay = -fy / tz2;
+        const float ay = -fy * itz2;
         const float u0sw2 = u0[0] * sw2[0] + u0[1] * sw2[1] + u0[2] * sw2[2];
         dp[1] += dl_db * (ay * u0sw2) + dl_dc * (2.0f * ay * w2su1);
         // d/dtz: dT row 0 = -fx/tz^2 W0 + 2 fx tx/tz^3 W2, row 1 = -fy/tz^2 W1 + 2 fy ty/tz^3 W2
         float g0[3], g1[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            g0[k] = (-fx / tz2) * V.m[0][k] + (2.0f * fx * tx / tz3) * V.m[2][k];
-            g1[k] = (-fy / tz2) * V.m[1][k] + (2.0f * fy * ty / tz3) * V.m[2][k];
+            g0[k] = ax * V.m[0][k] + (2.0f * fx * tx * itz3) * V.m[2][k];
+            g1[k] = ay * V.m[1][k] + (2.0f * fy * ty * itz3) * V.m[2][k];
         }
         const float g0su0 = g0[0] * su0[0] + g0[1] * su0[1] + g0[2] * su0[2];
         const float g0su1 = g0[0] * su1[0] + g0[1] * su1[1] + g0[2] * su1[2];
@@ -183,7 +186,8 @@ __global__ void __launch_bounds__(128, 8) k_geom_view(const float4* __restrict__
     const float ux = c.pos[0] - pos[0], uy = c.pos[1] - pos[1], uz = c.pos[2] - pos[2];
     const float len = sqrtf(ux * ux + uy * uy + uz * uz);
     if (len > 1e-8f && (mr != 0.0f || mg != 0.0f || mb != 0.0f)) {
-        const float dir[3] = {ux / len, uy / len, uz / len};
+        const float ilen = 1.0f / len;
+        const float dir[3] = {ux * ilen, uy * ilen, uz * ilen};
         float db[16][3];
         sh_basis_grad(dir, db);
         float dd0 = 0.0f, dd1 = 0.0f, dd2 = 0.0f;
@@ -202,9 +206,9 @@ __global__ void __launch_bounds__(128, 8) k_geom_view(const float4* __restrict__
             }
         }
         const float dot = dir[0] * dd0 + dir[1] * dd1 + dir[2] * dd2;
-        dpos[0] += -((dd0 - dir[0] * dot) / len);
-        dpos[1] += -((dd1 - dir[1] * dot) / len);
-        dpos[2] += -((dd2 - dir[2] * dot) / len);
+        dpos[0] += -((dd0 - dir[0] * dot) * ilen);
+        dpos[1] += -((dd1 - dir[1] * dot) * ilen);
+        dpos[2] += -((dd2 - dir[2] * dot) * ilen);
     }
     gv[s] = make_float4(dpos[0], dpos[1], dpos[2], a0.w);
     gv[S + s] = make_float4(dS[0], dS[1], dS[2], dS[3]);

@@ -205,8 +205,8 @@ __global__ void __launch_bounds__(256, 5) k_project(const float4* __restrict__ p
                 else hi |= b << (8 * (r - 8));
             }
         }
-        spans[s] = pack ? make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32))
-                        : make_uint4(SPANS_NONE, SPANS_NONE, SPANS_NONE, SPANS_NONE);
+        spans[2 * s] = pack ? make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32))
+                            : make_uint4(SPANS_NONE, SPANS_NONE, SPANS_NONE, SPANS_NONE);
     }
     cnt[s] = count;
     if (count) {
@@ -214,8 +214,12 @@ __global__ void __launch_bounds__(256, 5) k_project(const float4* __restrict__ p
         const unsigned m = __activemask();
         if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(visible, (uint32_t)__popc(m));
     }
-    tdesc[s] = make_uint2((uint32_t)(c.tile_base + cty0 * c.tiles_x + ctx0),
-                          (uint32_t)(ctx1 - ctx0) | ((uint32_t)(cty1 - cty0) << 16));
+    const uint2 td = make_uint2((uint32_t)(c.tile_base + cty0 * c.tiles_x + ctx0),
+                                (uint32_t)(ctx1 - ctx0) | ((uint32_t)(cty1 - cty0) << 16));
+    tdesc[s] = td;
+    // with prune, the tile rectangle again beside the spans: the tile-list
+    // masks gather one 32-byte record per entry
+    if (prune) spans[2 * s + 1] = make_uint4(td.x, td.y, 0u, 0u);
     dkey[s] = __float_as_uint(o.depth);
 }
 

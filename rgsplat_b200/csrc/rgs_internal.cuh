@@ -165,7 +165,7 @@ void launch_check_finite(const float4* planes, int n, int cap, int* flag, cudaSt
 // its CTA-tile rectangle), cnt[s] = its number of CTA tiles, or with prune = 1
 // the number inside the rows' kept spans (tiles.cuh); zero for culled slots.
 // *visible (zeroed by the caller) gains the number of slots with cnt > 0.
-// With prune, spans[slot] holds the kept spans of rectangles up to SPAN_ROWS
+// With prune, spans[2 slot] holds the kept spans of rectangles up to SPAN_ROWS
 // rows and 15 columns, byte r of the 16 (x holds rows 0-3, y 4-7, ...): first
 // kept column - first rectangle column | kept count << 4. Larger rectangles
 // get SPANS_NONE in every word (a byte 0xff never occurs in a packed record:
@@ -228,7 +228,7 @@ struct SupertileArgs {
     const uint32_t* ent_slot;      // sorted entries: slot
     const uint32_t* n_ent;         // device count of the sorted entries
     const uint2* tdesc;            // per slot: first CTA tile, rect width | height << 16
-    const uint4* spans;            // per slot (with prune): packed kept spans, or SPANS_NONE
+    const uint4* spans;            // per slot (with prune), 32 B: packed kept spans (or SPANS_NONE), then tdesc
     const float4* rec;             // splat records (three planes of S)
     uint32_t S;
     uint32_t n_per_view;           // slot = view * n_per_view + Gaussian

@@ -161,8 +161,18 @@ __global__ void __launch_bounds__(ST_THREADS, 4) k_st_masks(SupertileArgs a) {
 #pragma unroll
         for (int r = 0; r < ST_RUN; ++r) {
             const uint32_t e = e0 + (uint32_t)(ST_THREADS * r);
-            d[r] = e < n ? tdesc[slot[r]] : make_uint2(0u, 0u);
-            sp[r] = e < n && a.prune ? spans[slot[r]] : make_uint4(0u, 0u, 0u, 0u);
+            sp[r] = make_uint4(0u, 0u, 0u, 0u);
+            d[r] = make_uint2(0u, 0u);
+            if (e < n) {
+                if (a.prune) {
+                    // one 32-byte record: the spans, then the rectangle
+                    sp[r] = spans[2 * (size_t)slot[r]];
+                    const uint4 td = spans[2 * (size_t)slot[r] + 1];
+                    d[r] = make_uint2(td.x, td.y);
+                } else {
+                    d[r] = tdesc[slot[r]];
+                }
+            }
         }
         uint32_t acc[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
