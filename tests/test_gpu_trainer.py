@@ -146,10 +146,14 @@ def test_batch_past_pair_limit_runs_as_view_groups():
     assert sa.t == sb.t == len(steps)
     assert np.array_equal(sa.grad_denom, sb.grad_denom)
     # the accumulated screen-space gradient follows the parameters: where those
-    # took a different Adam step, it differs by a few percent
+    # took a different Adam step, it differs by a few percent. Which Gaussians
+    # those are depends on the rounding of near-zero gradients (float atomics
+    # order them differently run to run): 0 to 26 of the 4000 were measured
+    # over repeated runs, with the norm of the difference at most 1.1e-4 of
+    # the norm
     ga, gb = sa.grad_accum, sb.grad_accum
     close = np.isclose(gb, ga, rtol=1e-3, atol=1e-6 * float(np.abs(ga).max()))
-    assert close.mean() > 0.995, close.mean()
+    assert close.mean() > 0.99, close.mean()
     assert np.linalg.norm(ga - gb) <= 1e-2 * np.linalg.norm(ga)
     # gradients only (no Adam), on identical parameters: the groups' gradients are summed
     g3 = tp.gaussians()
