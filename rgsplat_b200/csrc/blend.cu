@@ -24,8 +24,10 @@
 //   * backward: per (warp, staged splat), the same test on the box of the
 //     warp's own strip of pixel rows; a warp whose strip the splat cannot
 //     reach skips it (warp-uniform). (The same skip in the forward measured
-//     slower: a skipped splat costs the forward little, and the branch cost
-//     more than it saved.)
+//     slower, as a per-splat branch and as a per-warp list of the needed
+//     splats alike: a pair that does not contribute costs the packed forward
+//     about five instructions per pixel, less than the strip tests add to
+//     every staging round.)
 //   * backward warps skip splats past the warp's largest last_contrib.
 // Backward pre-reduces each splat's 9 partial gradients across the warp with
 // shuffles (only when a lane contributed), across warps with shared-memory
