@@ -134,6 +134,29 @@ def test_pruned_lists_are_ordered_subsets_of_the_full_lists(ctx):
     assert np.array_equal(rgb.reshape(-1).view(np.uint32), orgb.reshape(-1).view(np.uint32))
 
 
+def test_supertile_entry_and_pair_counts(ctx):
+    """An unpruned render (non-zero background) bins every projected splat
+    once per CTA tile of its rectangle (rgs_stats.pairs) and once per 4x4-tile
+    supertile the rectangle meets (rgs_stats.supertile_entries): both counted
+    here from the projection's tile rectangles."""
+    g, cam, _ = small_scene(n=3000, seed=13, w=640, h=480)
+    g = g.copy()
+    g[:100, 7:10] += np.float32(np.log(6.0))  # some rectangles several supertiles wide
+    R.render_color(g, cam, (0.1, 0.1, 0.1), ctx=ctx)
+    st = ctx.stats()
+    vis, _, rect = D.project(g, cam, ctx)
+    tiles_x, tiles_y = -(-cam.width // 16), -(-cam.height // 16)
+    r = rect[vis != 0].astype(np.int64)
+    cx0, cy0 = r[:, 0], r[:, 1]
+    cx1, cy1 = np.minimum(r[:, 2], tiles_x), np.minimum(r[:, 3], tiles_y)
+    ok = (cx1 > cx0) & (cy1 > cy0)
+    cx0, cy0, cx1, cy1 = cx0[ok], cy0[ok], cx1[ok], cy1[ok]
+    assert st["pairs"] == int(((cx1 - cx0) * (cy1 - cy0)).sum())
+    entries = ((cx1 - 1) // 4 - cx0 // 4 + 1) * ((cy1 - 1) // 4 - cy0 // 4 + 1)
+    assert st["supertile_entries"] == int(entries.sum())
+    assert (entries > 1).sum() > 100
+
+
 def test_render_color_odd_sizes(ctx):
     g, cam, _ = small_scene(n=3000, seed=6, w=173, h=91, fx=200.0)
     rgb = R.render_color(g, cam, (0.1, 0.1, 0.1), ctx=ctx)
