@@ -289,11 +289,18 @@ __global__ void __launch_bounds__(BIN_THREADS) k_compact_visible(const uint32_t*
     __shared__ uint32_t s_w[BIN_THREADS / 32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t base = blockIdx.x * (uint32_t)CMP_CHUNK + threadIdx.x * CMP_PER;
+    // every slot's count, depth key and tile rectangle in one round trip
+    // (a culled slot's key and rectangle are read and dropped)
     bool f[CMP_PER];
+    uint32_t kv[CMP_PER];
+    uint2 dv[CMP_PER];
     uint32_t local = 0;
 #pragma unroll
     for (int k = 0; k < CMP_PER; ++k) {
-        f[k] = base + k < S && cnt[base + k] != 0u;
+        const bool in = base + k < S;
+        f[k] = in && cnt[base + k] != 0u;
+        kv[k] = in ? key[base + k] : 0u;
+        dv[k] = in ? tdesc[base + k] : make_uint2(0u, 0u);
         local += f[k] ? 1u : 0u;
     }
     uint32_t x = local;
@@ -311,12 +318,12 @@ __global__ void __launch_bounds__(BIN_THREADS) k_compact_visible(const uint32_t*
     for (int k = 0; k < CMP_PER; ++k) {
         if (f[k]) {
             const uint32_t slot = base + k;
-            ckey[pos] = key[slot];
+            ckey[pos] = kv[k];
             cslot[pos] = slot;
             ++pos;
             // the supertiles its tile rectangle meets
             const DevCam& c = cams[slot / n_per_view];
-            const uint2 d = tdesc[slot];
+            const uint2 d = dv[k];
             const int lt = (int)d.x - c.tile_base;
             const int ty0 = lt / c.tiles_x, cx0 = lt - ty0 * c.tiles_x;
             const int sx0 = cx0 / ST_EDGE, sx1 = (cx0 + (int)(d.y & 0xffffu) - 1) / ST_EDGE;
