@@ -14,7 +14,7 @@ src/pipeline/mod.rs:235-246): the batch's loss is the per-view losses and its
 gradient the sum of the per-view GaussianGrads of ``render_and_backward``
 (src/cpu/backward.rs:107-149), then one Adam step with grad_denom += 8. Bars:
 every view's rendered image and final transmittance bit-exact against the
-oracle's forward_pass (the north_star bar is 1e-4), dL/dpixel of the
+oracle's forward_pass (the stated image tolerance is 1e-4), dL/dpixel of the
 benchmarked (fused-tap) loss within float rounding of the reference's and
 bit-exact with exact_loss on the same images,
 per-view losses within 1e-4 of the same image's loss summed in double (the

@@ -8,7 +8,7 @@ per (pixel, splat) (src/cpu/backward.rs:344, :444), the SSIM window
 library's own deterministic routines, and the oracle by default with the same
 routines, which is what makes the other parity tests bit-exact. Here the
 oracle switches to glibc (``set_libm_math(True)``), i.e. to the reference's
-arithmetic, and the CUDA results are held to the north_star bars against it:
+arithmetic, and the CUDA results are held to the stated tolerances against it:
 
 * tile lists bit-exact except for entries whose 3-sigma rectangle flipped at a
   truncation boundary (counted, at most 1 per million pairs plus 2);

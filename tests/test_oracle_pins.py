@@ -3,7 +3,7 @@
 The reference ships no golden vectors; its inline ``#[cfg(test)]`` modules and
 ``tests/training_reduces_loss.rs`` are the only known answers. Each test below
 restates one of them (same inputs, same tolerance) against the oracle, so the
-oracle that later judges the CUDA path is itself held to the reference's bar.
+oracle that later checks the CUDA path is itself held to the reference's bar.
 """
 import math
 
