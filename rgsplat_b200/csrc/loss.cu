@@ -18,7 +18,9 @@
 // rgs_options.exact_loss); k_loss_fused, the default, accumulates with fused
 // multiply-adds on packed f32x2 pairs and forms the three SSIM quotients from
 // one reciprocal. The scalar loss is reduced per CTA and then per view in a
-// fixed order (deterministic).
+// fixed order (deterministic). (Staging each channel by 4-byte asynchronous
+// copies issued during the previous channel's passes 2-4, with the tile's
+// centre kept apart for pass 4, measured slower: 0.84 against 0.80 ms.)
 #include <mutex>
 
 #include "rgs_internal.cuh"
