@@ -256,7 +256,10 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_st_scan(SupertileArgs a) {
 // a lane scan of the byte counters.
 __global__ void __launch_bounds__(ST_THREADS) k_st_lists(SupertileArgs a) {
     __shared__ uint32_t s_w[ST_WARPS][4];
-    __shared__ unsigned long long s_base[ST_WARPS][ST_TILES];
+    // the warp's start in each plane, clamped to the capacity: every place
+    // formed from it then stays below 2^32 (cap <= 0xF0000000, the offsets
+    // below 256) and a clamped start still flags the overflow
+    __shared__ uint32_t s_base[ST_WARPS][ST_TILES];
     const uint32_t* __restrict__ ent_key = a.ent_key;
     const uint32_t* __restrict__ ent_slot = a.ent_slot;
     const uint16_t* __restrict__ masks = a.masks;
@@ -286,7 +289,7 @@ __global__ void __launch_bounds__(ST_THREADS) k_st_lists(SupertileArgs a) {
         if (lane < ST_TILES) {
             unsigned long long b = plane0 + a.chunk_cnt[(size_t)lane * a.chunk_stride + ch];
             for (int k = 0; k < w; ++k) b += byte_of(s_w[k][lane >> 2], lane & 3);
-            s_base[w][lane] = b;
+            s_base[w][lane] = (uint32_t)min(b, (unsigned long long)a.cap);
         }
         __syncwarp();
         uint32_t before[4] = {0u, 0u, 0u, 0u};  // the warp's earlier rounds, per byte (< 128)
@@ -318,7 +321,7 @@ __global__ void __launch_bounds__(ST_THREADS) k_st_lists(SupertileArgs a) {
                 while (nib) {
                     const int j = __ffs(nib) - 1;
                     nib &= nib - 1u;
-                    const unsigned long long at = s_base[w][4 * k + j] + byte_of(excl[k], j);
+                    const uint32_t at = s_base[w][4 * k + j] + byte_of(excl[k], j);
                     if (at < a.cap) a.vals_out[at] = slot[r];
                     else *a.overflow = 1;
                 }
@@ -342,10 +345,10 @@ __global__ void __launch_bounds__(ST_THREADS) k_st_lists(SupertileArgs a) {
                 for (int t = 0; t < ST_TILES; ++t) {
                     const int tx = sx * ST_EDGE + t % ST_EDGE, ty = sy * ST_EDGE + t / ST_EDGE;
                     if (tx < c.tiles_x && ty < c.tiles_y) {
-                        const unsigned long long at = s_base[w][t] + byte_of(excl[t >> 2], t & 3);
+                        const uint32_t at = s_base[w][t] + byte_of(excl[t >> 2], t & 3);
                         uint32_t* rg = reinterpret_cast<uint32_t*>(a.ranges + (c.tile_base + ty * c.tiles_x + tx));
-                        if (first) rg[0] = (uint32_t)min(at, (unsigned long long)a.cap);
-                        if (last) rg[1] = (uint32_t)min(at + ((m[r] >> t) & 1u), (unsigned long long)a.cap);
+                        if (first) rg[0] = min(at, a.cap);
+                        if (last) rg[1] = min(at + ((m[r] >> t) & 1u), a.cap);
                     }
                 }
             }
