@@ -8,18 +8,21 @@
 // chunks of ST_CHUNK, whatever supertiles they belong to, so every CTA gets
 // the same work however unevenly the splats crowd the supertiles:
 //   k_st_masks: per entry, the tiles of its supertile the slot keeps (the
-//               rectangle, or with pruning each tile row's kept span: the same
-//               test on the same floats the projection counted with) as a
-//               16-bit mask, bit t for tile position t = row * ST_EDGE + col;
-//               per chunk and position, the entries with that bit set;
+//               rectangle, or with pruning each tile row's kept span, read
+//               from the spans the projection packed in the slot's 32-byte
+//               record, or for rectangles too large to pack recomputed by
+//               the same test on the same floats the projection counted
+//               with) as a 16-bit mask, bit t for tile position
+//               t = row * ST_EDGE + col; per chunk and position, the entries
+//               with that bit set (packed byte counters);
 //   k_st_scan:  one CTA per position: an exclusive scan of its chunk counts;
 //   k_st_lists: the lists. The pairs of position t form plane t of the list
 //               buffer, in entry order, the planes one after another; the
 //               list of a tile (the entries of one supertile with bit t) is
 //               then one contiguous run of its plane. An entry's place in
 //               plane t is the plane's start + its chunk's scanned count + the
-//               entries before it in the chunk with bit t (one ballot per
-//               position per 32 entries). The first and the last entry of each
+//               entries before it in the chunk with bit t (a lane scan of the
+//               byte counters). The first and the last entry of each
 //               supertile write the [start, end) of its tiles.
 // The supertile sort is stable and its input is in depth order, so each list
 // holds its splats in depth order with ties in slot order: the lists the
