@@ -407,7 +407,9 @@ __global__ void __launch_bounds__(128, PART == 2 ? 8 : 6) k_geom_gauss(const flo
 // of two per view; the sums run in view order as before. (Loading all four
 // planes' parameters and moments before the first store as well needed 104
 // registers and ran slower at the lower occupancy; two planes at a time ran
-// slower too, at 74 registers and 6 CTAs per SM or 64 with spills at 8.)
+// slower too, at 74 registers and 6 CTAs per SM or 64 with spills at 8; and
+// one thread per plane, twelve per Gaussian each repeating the view loop,
+// took 1.2 against 0.93 ms for the stage.)
 constexpr int VIEW_GROUP = 8;
 __global__ void __launch_bounds__(128, 8) k_geom_sh(int n, int cap, const DevCam* __restrict__ cams, int nviews,
                                                    const uint32_t* __restrict__ cnt, const float4* __restrict__ gv, AdamArgs a) {
