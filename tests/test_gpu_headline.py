@@ -5,8 +5,9 @@ per step drawn by the reference's xorshift camera schedule from 128
 Fibonacci-sphere cameras of 1600x1064, 1280x720 and 960x540 pixels: the step
 the benchmark times, in the blend layout it tunes to (16x16 tiles, 128-splat
 batches, 2 pixels per thread). At this size the batched pipeline runs paths no
-smaller test reaches: ~50k CTA tiles over the batch (16-bit global tile ids,
-two tile-sort passes), ~70M (tile, splat) pairs after pruning, ~8.5M pixels at
+smaller test reaches: ~50k CTA tiles over the batch (16-bit global tile ids),
+~3.4k supertiles (two 8-bit passes of the supertile sort) over ~16M (supertile,
+splat) entries, ~66M (tile, splat) pairs after pruning, ~8.5M pixels at
 per-view offsets in one buffer.
 
 Multi-view semantics (the reference trains one view per step,
@@ -79,7 +80,12 @@ def test_headline_batch_shape(headline):
     assert st["view_groups"] == 1
     assert st["pairs"] > 1 << 25
     tiles = sum(((cfg.cameras[v].width + 15) // 16) * ((cfg.cameras[v].height + 15) // 16) for v in views)
-    assert tiles > 1 << 15  # 16-bit global tile ids: two 8-bit tile-sort passes
+    assert tiles > 1 << 15  # 16-bit global tile ids
+    # more supertiles than one 8-bit sort pass orders, each splat binned once per
+    # supertile it meets (fewer entries than pairs)
+    supertiles = sum(((cfg.cameras[v].width + 63) // 64) * ((cfg.cameras[v].height + 63) // 64) for v in views)
+    assert supertiles > 1 << 8
+    assert st["visible"] < st["supertile_entries"] < st["pairs"]
 
 
 def test_headline_images_bit_exact_and_pixel_gradients(headline):
