@@ -231,13 +231,16 @@ def profiled_traffic(kernel_file: str):
         return None
 
 
-def profiled_issue_active(kernel_prefix: str):
-    """Fraction of issue slots a kernel kept busy, from the committed ncu table
-    of the step's kernels (half-size capture of the same launch shape)."""
+def profiled_issue_active(kernel: str):
+    """Fraction of issue slots the packed blend kernel kept busy, from the
+    committed ncu pipe-mix table (quarter-size capture of the same launch
+    shape; columns: forward scalar, forward packed, backward scalar, backward
+    packed)."""
+    col = {"k_blend_fwd": 3, "k_blend_bwd": 5}.get(kernel)
     try:
-        for line in open(os.path.join(ROOT, "profiles", "step_kernels_500k_8views.md")):
-            if line.startswith(f"| `{kernel_prefix}"):
-                return round(float(line.split("|")[5]) / 100.0, 3)
+        for line in open(os.path.join(ROOT, "profiles", "blend_pipes_250k_8views.md")):
+            if col and line.startswith("| issue slots active |"):
+                return round(float(line.split("|")[col].strip().rstrip("%").strip()) / 100.0, 3)
     except (OSError, ValueError, IndexError):
         pass
     return None
@@ -687,7 +690,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                                                                 f"x 2 x {clock_mhz:.0f} MHz (median sampled SM clock)"},
                     "issue_active": profiled_issue_active("k_blend_bwd") if dom == "backward" else None,
                     "note": "the blend kernels are bound by instruction issue, not DRAM (issue_active: fraction of issue "
-                            "slots busy, ncu, profiles/step_kernels_500k_8views.md); fp32 is the roof that applies, "
+                            "slots busy, ncu, profiles/blend_pipes_250k_8views.md); fp32 is the roof that applies, "
                             "the HBM fraction is reported as the contract asks"}
 
     cpu = None
